@@ -1,0 +1,208 @@
+/*
+ * pico_gpu.h -- C ABI of the B200 trace-commitment path.
+ *
+ * The reference prover (brevis-network/pico) commits traces through Plonky3's
+ * trait objects, selected by type aliases in its STARK configs:
+ *   SC_Dft = Radix2DitParallel, SC_ValMmcs = MerkleTreeMmcs<..Poseidon2..>,
+ *   SC_Pcs = TwoAdicFriPcs  (vm/src/configs/stark_config/kb_poseidon2.rs:15-27,
+ *   bb_poseidon2.rs:15-27; PCS constructed at kb_poseidon2.rs:82-93).
+ * A GPU-backed config swaps those aliases for Rust types whose methods call
+ * the entry points below; the prover's call sites stay unchanged
+ * (pcs.commit: vm/src/machine/prover.rs:102,244,415,540;
+ *  get_evaluations_on_domain: prover.rs:469-489; pcs.open: prover.rs:589).
+ *
+ * Conventions
+ *   - Field elements are u32 in Plonky3's Montgomery form (x * 2^32 mod p), the
+ *     in-memory representation of KoalaBear / BabyBear (MontyField31), so Rust
+ *     `Vec<KoalaBear>` buffers pass through without conversion.
+ *   - Matrices are row-major, height = 2^log_height rows of `width` elements
+ *     (RowMajorMatrix).
+ *   - Every function returns a pico_status; nothing aborts, nothing throws
+ *     across the boundary (precedent: the reference's own C ABI,
+ *     gnark/field-ffi/src/koalabear.rs:6-21).  pico_gpu_last_error() returns a
+ *     thread-local description of the last failure.
+ *   - All functions are thread-safe; concurrent calls on one context overlap
+ *     on the device (the reference commits chunks from rayon workers,
+ *     vm/src/instances/machine/riscv.rs:234).
+ */
+#ifndef PICO_GPU_H
+#define PICO_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PICO_GPU_ABI_VERSION 1u
+
+typedef enum {
+  PICO_OK = 0,
+  PICO_ERR_INVALID_ARG = 1,
+  PICO_ERR_OUT_OF_MEMORY = 2, /* device allocation failed or HBM budget exceeded */
+  PICO_ERR_CUDA = 3,
+  PICO_ERR_UNSUPPORTED = 4,
+  PICO_ERR_TIMEOUT = 5,
+  PICO_ERR_NOT_READY = 6, /* asynchronous request still in flight */
+  PICO_ERR_CANCELLED = 7,
+  PICO_ERR_NO_DEVICE = 8
+} pico_status;
+
+typedef enum { PICO_KOALABEAR = 0, PICO_BABYBEAR = 1 } pico_field;
+
+/* Flags for commit / LDE / FRI calls. */
+#define PICO_INPUT_DEVICE 0x1u /* input pointers are device pointers (else host) */
+#define PICO_COMMIT_PLAIN 0x2u /* one matrix per launch, no graph: the baseline form */
+#define PICO_OUTPUT_DEVICE 0x4u /* output pointers are device pointers (else host) */
+#define PICO_LDE_NATURAL_ORDER 0x8u /* coset_lde_batch: natural row order (Dft trait); default bit-reversed */
+
+typedef struct pico_ctx pico_ctx;
+/* Prover data of one commit: every LDE and every digest layer stays resident
+ * on the device until pico_gpu_release (the Rust ProverData's Drop). */
+typedef struct pico_commit pico_commit;
+/* Resident layers of one FRI commit phase (codewords and their trees). */
+typedef struct pico_fri pico_fri;
+/* An asynchronous commit request (serving path). */
+typedef struct pico_request pico_request;
+
+typedef struct {
+  const uint32_t *values; /* row-major 2^log_height x width, Monty form */
+  uint32_t log_height;
+  uint32_t width;
+  uint32_t shift; /* LDE coset shift, Monty form: GENERATOR / domain.shift */
+  uint32_t reserved;
+} pico_matrix;
+
+typedef struct {
+  uint64_t hbm_budget_bytes; /* admission budget; 0 = 90% of free HBM at init */
+  uint32_t n_streams;        /* device streams for concurrent requests; 0 = 8 */
+  uint32_t flags;
+  uint32_t reserved[6];
+} pico_config;
+
+/* Device-side timing and work counts of one commit, from CUDA events recorded
+ * on the commit's stream (milliseconds). */
+typedef struct {
+  double total_ms;   /* first input copy or launch -> root ready */
+  double h2d_ms;     /* host -> device input copies (host inputs only) */
+  double lde_ms;     /* coset LDE kernels, all matrices */
+  double leaves_ms;  /* leaf hashing of the tallest height group */
+  double tree_ms;    /* compression levels, including injected rows */
+  uint64_t cells;    /* trace cells before blowup */
+  uint64_t lde_cells;
+  uint64_t permutations; /* Poseidon2 permutations in the tree */
+  uint64_t leaf_permutations;
+  uint64_t lde_bytes; /* algorithmic LDE bytes: 4 * (cells + lde_cells) */
+  uint64_t launches;  /* kernels this library launched for the commit */
+} pico_commit_stats;
+
+/* Duplex challenger state, DuplexChallenger<F, Perm, 16, 8> (Monty form). */
+typedef struct {
+  uint32_t sponge[16];
+  uint32_t in_buf[8];
+  uint32_t in_len;
+  uint32_t out_buf[8];
+  uint32_t out_len;
+} pico_challenger;
+
+/* ---- context ------------------------------------------------------------ */
+pico_status pico_gpu_init(int device, const pico_config *cfg, pico_ctx **out);
+pico_status pico_gpu_shutdown(pico_ctx *ctx);
+const char *pico_gpu_last_error(void);
+uint32_t pico_gpu_abi_version(void);
+/* Bytes currently reserved by resident commits / in-flight requests, and the budget. */
+pico_status pico_gpu_memory(pico_ctx *ctx, uint64_t *reserved, uint64_t *budget);
+
+/* ---- Pcs::commit ---------------------------------------------------------
+ * TwoAdicFriPcs::commit (Plonky3 @ brevis-network/Plonky3 f5056c9, called at
+ * vm/src/machine/prover.rs:102,244,415,540): per matrix a coset LDE with
+ * log_blowup and the matrix's shift, rows bit-reversed, then one
+ * MerkleTreeMmcs commit over all LDEs (stable sort by height, rows of shorter
+ * matrices injected at their level).  Heights must be powers of two.
+ * `out` (nullable) receives the resident prover data; root receives the
+ * 8-element commitment (host memory). */
+pico_status pico_gpu_commit(pico_ctx *ctx, pico_field field, const pico_matrix *mats, uint32_t n_mats,
+                            uint32_t log_blowup, uint32_t flags, pico_commit **out, uint32_t root[8]);
+pico_status pico_gpu_release(pico_ctx *ctx, pico_commit *c);
+/* Timing of a finished commit (waits for it), and of the last synchronous
+ * commit made by the calling thread (also when its prover data was not kept). */
+pico_status pico_gpu_commit_stats(const pico_commit *c, pico_commit_stats *out);
+pico_status pico_gpu_last_commit_stats(pico_commit_stats *out);
+
+/* Pcs::get_evaluations_on_domain / open_batch row reads (prover.rs:469-489):
+ * rows [row_begin, row_end) of committed LDE `mat_idx` (input order), in the
+ * committed (bit-reversed) row order.  Output is host memory unless
+ * PICO_OUTPUT_DEVICE. */
+pico_status pico_gpu_lde_rows(pico_ctx *ctx, const pico_commit *c, uint32_t mat_idx, uint64_t row_begin,
+                              uint64_t row_end, uint32_t *out, uint32_t flags);
+/* Shape of a committed LDE: log2 height and width. */
+pico_status pico_gpu_lde_shape(const pico_commit *c, uint32_t mat_idx, uint32_t *log_height, uint32_t *width);
+/* Digest layer `level` (0 = leaves) of the commit's tree: 2^(log_max - level)
+ * digests of 8 words. */
+pico_status pico_gpu_digest_layer(pico_ctx *ctx, const pico_commit *c, uint32_t level, uint32_t *out,
+                                  uint32_t flags);
+/* Mmcs::open_batch: the opened rows of every matrix at `index` (an index into
+ * the tallest LDE; shorter matrices use index >> (log_max - log_h)) and the
+ * sibling path.  rows_out receives the concatenated rows in input order
+ * (sum of widths words); path_out receives log_max digests of 8 words. */
+pico_status pico_gpu_open_batch(pico_ctx *ctx, const pico_commit *c, uint64_t index, uint32_t *rows_out,
+                                uint32_t *path_out);
+
+/* ---- Dft / Mmcs / permutation granularity -------------------------------- */
+/* Radix2DitParallel::coset_lde_batch (SC_Dft, kb_poseidon2.rs:25): n x w
+ * evaluations on the two-adic subgroup -> 2^log_blowup * n evaluations on
+ * shift * H, bit-reversed rows unless PICO_LDE_NATURAL_ORDER. */
+pico_status pico_gpu_coset_lde_batch(pico_ctx *ctx, pico_field field, const uint32_t *in, uint32_t log_n,
+                                     uint32_t width, uint32_t log_blowup, uint32_t shift, uint32_t *out,
+                                     uint32_t flags);
+/* MerkleTreeMmcs::commit (SC_ValMmcs, kb_poseidon2.rs:19-20) over matrices
+ * that are already extended: mats[i].log_height is the matrix's own height,
+ * shift is ignored. */
+pico_status pico_gpu_mmcs_commit(pico_ctx *ctx, pico_field field, const pico_matrix *mats, uint32_t n_mats,
+                                 uint32_t flags, pico_commit **out, uint32_t root[8]);
+/* Poseidon2KoalaBear<16> / Poseidon2BabyBear<16> on n states of 16 words, in place. */
+pico_status pico_gpu_poseidon2_permute(pico_ctx *ctx, pico_field field, uint32_t *states, uint64_t n,
+                                       uint32_t flags);
+
+/* ---- FRI commit phase (inside TwoAdicFriPcs::open, prover.rs:589) ----------
+ * codeword: 2^log_n degree-4 extension elements (4 words each, c0..c3), in
+ * bit-reversed evaluation order.  Rounds: commit the codeword as a
+ * (len/2) x 2 extension matrix flattened to 8 base columns (ExtensionMmcs),
+ * observe the root, sample beta (sample_ext), fold with arity 2; stop at
+ * length 2^(log_blowup + log_final_len).  If betas_in is non-null the round
+ * challenges are taken from it (rounds x 4 words) instead of the challenger.
+ * ch (in/out, used when betas_in is null) is the prover's challenger state.
+ * Outputs (host): roots (rounds x 8), betas (rounds x 4), final_out
+ * (2^log_final_len x 4: with log_final_len = 0 the single final_poly element).
+ * `out` (nullable) keeps every codeword and tree resident for queries. */
+pico_status pico_gpu_fri_commit_phase(pico_ctx *ctx, pico_field field, const uint32_t *codeword, uint32_t log_n,
+                                      uint32_t log_blowup, uint32_t log_final_len, const uint32_t *betas_in,
+                                      pico_challenger *ch, uint32_t flags, uint32_t *roots, uint32_t *betas,
+                                      uint32_t *final_out, uint32_t *n_rounds, pico_fri **out);
+pico_status pico_gpu_fri_release(pico_ctx *ctx, pico_fri *f);
+/* Codeword of round r (r = 0 is the input) as 2^(log_n - r) x 4 words. */
+pico_status pico_gpu_fri_layer(pico_ctx *ctx, const pico_fri *f, uint32_t round, uint32_t *out, uint32_t flags);
+
+/* ---- serving: asynchronous commits ----------------------------------------
+ * pico_gpu_submit_commit copies the host matrices it is given before it
+ * returns (the caller may reuse them) and queues the commit.  A request is
+ * admitted to the device when the HBM budget has room for its LDEs, digest
+ * layers and scratch; admitted requests run concurrently on separate streams.
+ * pico_gpu_wait blocks up to timeout_ms (< 0: forever) for completion and then
+ * hands over the prover data and root exactly as pico_gpu_commit would. */
+pico_status pico_gpu_submit_commit(pico_ctx *ctx, pico_field field, const pico_matrix *mats, uint32_t n_mats,
+                                   uint32_t log_blowup, uint32_t flags, pico_request **out);
+pico_status pico_gpu_poll(pico_ctx *ctx, pico_request *req);
+pico_status pico_gpu_wait(pico_ctx *ctx, pico_request *req, int64_t timeout_ms, pico_commit **out,
+                          uint32_t root[8]);
+/* Cancel a request that has not been admitted yet; admitted requests finish. */
+pico_status pico_gpu_cancel(pico_ctx *ctx, pico_request *req);
+/* Timing of a finished request: queue wait and device time in microseconds. */
+pico_status pico_gpu_request_times(const pico_request *req, double *queued_us, double *run_us);
+pico_status pico_gpu_request_free(pico_ctx *ctx, pico_request *req);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PICO_GPU_H */

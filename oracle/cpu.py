@@ -1,0 +1,201 @@
+"""ctypes wrapper of the C oracle (oracle/oracle.c) -- test infrastructure.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker or the timed CPU baseline; the product never does.
+All arrays are numpy uint32 in Montgomery form unless a name says canonical.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+import threading
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+_lib = None
+_lock = threading.Lock()
+
+
+class Challenger(C.Structure):
+    _fields_ = [
+        ("sponge", C.c_uint32 * 16),
+        ("in_buf", C.c_uint32 * 8),
+        ("in_len", C.c_uint32),
+        ("out_buf", C.c_uint32 * 8),
+        ("out_len", C.c_uint32),
+    ]
+
+
+def build(force: bool = False) -> Path:
+    srcs = [HERE / "oracle.c", HERE / "oracle.h", HERE.parent / "pico_b200" / "csrc" / "p2_rc_table.inc"]
+    if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"], check=True, capture_output=True)
+    return LIB
+
+
+def load():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            lib = C.CDLL(str(LIB))
+            u32, vp, u64 = C.c_uint32, C.c_void_p, C.c_uint64
+            for name, res, args in [
+                ("orc_prime", u32, [C.c_int]),
+                ("orc_to_monty", u32, [C.c_int, u32]),
+                ("orc_from_monty", u32, [C.c_int, u32]),
+                ("orc_two_adic_generator", u32, [C.c_int, u32]),
+                ("orc_generator", u32, [C.c_int]),
+                ("orc_num_threads", C.c_int, []),
+                ("orc_set_threads", None, [C.c_int]),
+                ("orc_permute", C.c_int, [C.c_int, vp, C.c_size_t]),
+                ("orc_permute_canonical", C.c_int, [C.c_int, vp]),
+                ("orc_hash", C.c_int, [C.c_int, vp, C.c_size_t, vp]),
+                ("orc_compress", C.c_int, [C.c_int, vp, vp, vp]),
+                ("orc_mmcs_commit", C.c_int, [C.c_int, u32, vp, vp, vp, vp, vp]),
+                ("orc_coset_lde", C.c_int, [C.c_int, vp, u32, u32, u32, u32, C.c_int, vp]),
+                ("orc_pcs_commit", C.c_int, [C.c_int, u32, vp, vp, vp, vp, u32, vp, vp, vp]),
+                ("orc_challenger_init", None, [C.POINTER(Challenger)]),
+                ("orc_challenger_observe", None, [C.c_int, C.POINTER(Challenger), u32]),
+                ("orc_challenger_sample", u32, [C.c_int, C.POINTER(Challenger)]),
+                ("orc_fri_commit_phase", C.c_int,
+                 [C.c_int, vp, u32, u32, u32, vp, C.POINTER(Challenger), vp, vp, vp, vp]),
+                ("orc_ext_mul", None, [C.c_int, vp, vp, vp]),
+            ]:
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+        return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise RuntimeError(f"oracle {what} failed with code {rc}")
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def set_threads(n: int):
+    load().orc_set_threads(n)
+
+
+def num_threads() -> int:
+    return load().orc_num_threads()
+
+
+def permute_canonical(field: int, state) -> np.ndarray:
+    s = _u32(state).copy()
+    _check(load().orc_permute_canonical(field, s.ctypes.data), "permute")
+    return s
+
+
+def permute(field: int, states) -> np.ndarray:
+    s = _u32(states).copy()
+    _check(load().orc_permute(field, s.ctypes.data, s.size // 16), "permute")
+    return s
+
+
+def hash_elems(field: int, elems) -> np.ndarray:
+    a = _u32(elems)
+    out = np.zeros(8, dtype=np.uint32)
+    _check(load().orc_hash(field, a.ctypes.data if a.size else None, a.size, out.ctypes.data), "hash")
+    return out
+
+
+def compress(field: int, left, right) -> np.ndarray:
+    l, r = _u32(left), _u32(right)
+    out = np.zeros(8, dtype=np.uint32)
+    _check(load().orc_compress(field, l.ctypes.data, r.ctypes.data, out.ctypes.data), "compress")
+    return out
+
+
+def mmcs_commit(field: int, mats, want_layers: bool = False):
+    mats = [_u32(m) for m in mats]
+    n = len(mats)
+    ptrs = (C.c_void_p * n)(*[m.ctypes.data for m in mats])
+    heights = np.array([m.shape[0] for m in mats], dtype=np.uint64)
+    widths = np.array([m.shape[1] for m in mats], dtype=np.uint32)
+    root = np.zeros(8, dtype=np.uint32)
+    layers = None
+    if want_layers:
+        hmax = int(heights.max())
+        layers = np.zeros(((2 * hmax - 1), 8), dtype=np.uint32)
+    _check(load().orc_mmcs_commit(field, n, ptrs, heights.ctypes.data, widths.ctypes.data, root.ctypes.data,
+                                  layers.ctypes.data if layers is not None else None), "mmcs_commit")
+    return (root, layers) if want_layers else root
+
+
+def coset_lde(field: int, mat, log_blowup: int, shift_monty: int, bitrev: bool = True) -> np.ndarray:
+    m = _u32(mat)
+    n, w = m.shape
+    logn = n.bit_length() - 1
+    out = np.zeros((n << log_blowup, w), dtype=np.uint32)
+    _check(load().orc_coset_lde(field, m.ctypes.data, logn, w, log_blowup, shift_monty, int(bitrev),
+                                out.ctypes.data), "coset_lde")
+    return out
+
+
+def pcs_commit(field: int, mats, shifts, log_blowup: int, want_ldes: bool = False, want_layers: bool = False):
+    mats = [_u32(m) for m in mats]
+    n = len(mats)
+    ptrs = (C.c_void_p * n)(*[m.ctypes.data for m in mats])
+    logh = np.array([m.shape[0].bit_length() - 1 for m in mats], dtype=np.uint32)
+    widths = np.array([m.shape[1] for m in mats], dtype=np.uint32)
+    sh = _u32(shifts)
+    root = np.zeros(8, dtype=np.uint32)
+    ldes = None
+    ldep = None
+    if want_ldes:
+        ldes = [np.zeros((m.shape[0] << log_blowup, m.shape[1]), dtype=np.uint32) for m in mats]
+        ldep = (C.c_void_p * n)(*[l.ctypes.data for l in ldes])
+    layers = None
+    if want_layers:
+        hmax = max(m.shape[0] for m in mats) << log_blowup
+        layers = np.zeros((2 * hmax - 1, 8), dtype=np.uint32)
+    _check(load().orc_pcs_commit(field, n, ptrs, logh.ctypes.data, widths.ctypes.data, sh.ctypes.data, log_blowup,
+                                 root.ctypes.data, ldep, layers.ctypes.data if layers is not None else None),
+           "pcs_commit")
+    return root, ldes, layers
+
+
+def new_challenger() -> Challenger:
+    ch = Challenger()
+    load().orc_challenger_init(C.byref(ch))
+    return ch
+
+
+def challenger_observe(field: int, ch: Challenger, v: int):
+    load().orc_challenger_observe(field, C.byref(ch), v)
+
+
+def challenger_sample(field: int, ch: Challenger) -> int:
+    return load().orc_challenger_sample(field, C.byref(ch))
+
+
+def fri_commit_phase(field: int, codeword, log_blowup: int, log_final_len: int = 0, betas=None, challenger=None):
+    cw = _u32(codeword)
+    log_n = cw.shape[0].bit_length() - 1
+    rounds = log_n - log_blowup - log_final_len
+    roots = np.zeros((max(rounds, 1), 8), dtype=np.uint32)
+    out_betas = np.zeros((max(rounds, 1), 4), dtype=np.uint32)
+    final = np.zeros((1 << log_final_len, 4), dtype=np.uint32)
+    ch = challenger if challenger is not None else new_challenger()
+    b = _u32(betas) if betas is not None else None
+    nr = C.c_uint32()
+    _check(load().orc_fri_commit_phase(field, cw.ctypes.data, log_n, log_blowup, log_final_len,
+                                       b.ctypes.data if b is not None else None, C.byref(ch), roots.ctypes.data,
+                                       out_betas.ctypes.data, final.ctypes.data, C.byref(nr)), "fri_commit_phase")
+    return roots[:rounds], out_betas[:rounds], final, ch
+
+
+def ext_mul(field: int, a, b) -> np.ndarray:
+    x, y = _u32(a), _u32(b)
+    out = np.zeros(4, dtype=np.uint32)
+    load().orc_ext_mul(field, x.ctypes.data, y.ctypes.data, out.ctypes.data)
+    return out

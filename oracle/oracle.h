@@ -1,0 +1,121 @@
+/*
+ * CPU oracle for the trace-commitment path: test infrastructure only.
+ *
+ * A plain-C restatement of the reference's hot-path arithmetic (Plonky3 as
+ * pinned by brevis-network/pico, restated from the Pico-owned files cited in
+ * oracle.c).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg may load it, and only as the checker or the timed CPU baseline; the
+ * product library never links it.
+ *
+ * All buffers at this interface hold field elements in Plonky3's Montgomery
+ * form (x * 2^32 mod p, the MontyField31 storage), exactly as the prover hands
+ * them over.  Internally the oracle computes in canonical form with plain
+ * 64-bit remainder arithmetic, so it shares no reduction tricks with the GPU.
+ *
+ * Parity status: the Poseidon2 permutation is pinned by the reference's
+ * known-answer tests (gnark/poseidon2/poseidon2_{koalabear,babybear}_test.go).
+ * Sponge, compression, mixed-height MMCS, FRI fold and challenger follow the
+ * reference's verifier restatements.  The two-adic generators are derived
+ * (GENERATOR^((p-1)/2^S)); no reference file pins them.
+ */
+#ifndef PICO_ORACLE_H
+#define PICO_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_KOALABEAR = 0, ORC_BABYBEAR = 1 };
+
+/* Return codes. */
+enum { ORC_OK = 0, ORC_EINVAL = 1, ORC_ENOMEM = 2 };
+
+/* Duplex challenger state (Monty form), DuplexChallenger<F, Perm, 16, 8>. */
+typedef struct {
+    uint32_t sponge[16];
+    uint32_t in_buf[8];
+    uint32_t in_len;
+    uint32_t out_buf[8];
+    uint32_t out_len;
+} orc_challenger;
+
+uint32_t orc_prime(int field);
+uint32_t orc_to_monty(int field, uint32_t x);
+uint32_t orc_from_monty(int field, uint32_t x);
+/* two_adic_generator(bits) in canonical form. */
+uint32_t orc_two_adic_generator(int field, uint32_t bits);
+uint32_t orc_generator(int field);
+int orc_num_threads(void);
+void orc_set_threads(int n);
+
+/* In-place Poseidon2-16 on n states (Monty form). */
+int orc_permute(int field, uint32_t *states, size_t n);
+/* In-place Poseidon2-16 on one state in canonical form (for KATs). */
+int orc_permute_canonical(int field, uint32_t state[16]);
+
+/* PaddingFreeSponge<16,8,8> over `len` Monty elements -> 8-element digest. */
+int orc_hash(int field, const uint32_t *in, size_t len, uint32_t out[8]);
+/* TruncatedPermutation<2,8,16>: permute(left || right)[0..8]. */
+int orc_compress(int field, const uint32_t left[8], const uint32_t right[8], uint32_t out[8]);
+
+/*
+ * MerkleTreeMmcs::commit over matrices of power-of-two heights (row-major,
+ * Monty).  `layers` (nullable) receives every digest layer from the leaves up
+ * to the root, concatenated: (2*H_max - 1) * 8 words.
+ */
+int orc_mmcs_commit(int field, uint32_t n_mats, const uint32_t *const *mats,
+                    const uint64_t *heights, const uint32_t *widths,
+                    uint32_t root[8], uint32_t *layers);
+
+/*
+ * Radix2DitParallel::coset_lde_batch: n = 2^log_n evaluations on the two-adic
+ * subgroup (row-major n x w) -> evaluations on shift * H_{n*2^b}.  If
+ * bitrev_rows is nonzero the rows are bit-reversed as TwoAdicFriPcs::commit
+ * does before hashing.
+ */
+int orc_coset_lde(int field, const uint32_t *in, uint32_t log_n, uint32_t w,
+                  uint32_t log_blowup, uint32_t shift_monty, int bitrev_rows,
+                  uint32_t *out);
+
+/*
+ * TwoAdicFriPcs::commit: per matrix coset LDE with shift = GENERATOR /
+ * domain_shift (passed precomputed in `shifts`, Monty), bit-reversed rows,
+ * then one MMCS commit over all.  `ldes` (nullable array of n_mats pointers)
+ * receives each LDE; `layers` as in orc_mmcs_commit.
+ */
+int orc_pcs_commit(int field, uint32_t n_mats, const uint32_t *const *mats,
+                   const uint32_t *log_heights, const uint32_t *widths,
+                   const uint32_t *shifts, uint32_t log_blowup,
+                   uint32_t root[8], uint32_t *const *ldes, uint32_t *layers);
+
+void orc_challenger_init(orc_challenger *ch);
+void orc_challenger_observe(int field, orc_challenger *ch, uint32_t v);
+uint32_t orc_challenger_sample(int field, orc_challenger *ch);
+
+/*
+ * FRI commit phase on one degree-4 extension codeword (N = 2^log_n rows of 4
+ * Monty words, bit-reversed evaluation order).  Folds with arity 2 until the
+ * length is 2^(log_blowup + log_final_len).  Per round: commit the codeword as
+ * an (N/2) x 2 extension matrix (flattened to 8 base columns), observe the
+ * root, sample beta (or take betas_in[round] if betas_in is non-null), fold.
+ * With log_final_len == 0 the result is Plonky3's single final_poly element
+ * (observed into the challenger); otherwise the 2^log_final_len coefficients.
+ * Outputs: roots (rounds x 8), betas (rounds x 4), final_out (2^log_final_len
+ * x 4, coefficients).  Returns the number of rounds via *rounds_out.
+ */
+int orc_fri_commit_phase(int field, const uint32_t *codeword, uint32_t log_n,
+                         uint32_t log_blowup, uint32_t log_final_len,
+                         const uint32_t *betas_in, orc_challenger *ch,
+                         uint32_t *roots, uint32_t *betas, uint32_t *final_out,
+                         uint32_t *rounds_out);
+
+/* Extension-field helpers (Monty in/out), for tests. */
+void orc_ext_mul(int field, const uint32_t a[4], const uint32_t b[4], uint32_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,790 @@
+// C-ABI implementation: context, device memory accounting, commit planning
+// and orchestration, LDE / MMCS / permutation entry points, FRI commit phase.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "field.cuh"
+#include "internal.h"
+#include "runtime.h"
+#include "serving.h"
+
+using namespace pico;
+
+namespace pico {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+pico_status cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return PICO_OK;
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  return PICO_ERR_CUDA;
+}
+
+static const uint32_t RC_RAW[30][16] = {
+#include "p2_rc_table.inc"
+};
+
+template <class F>
+static void host_p2_constants(uint32_t ext[8][16], uint32_t inte[24], uint32_t diag[16]) {
+  using B = Fp<F>;
+  const uint32_t p = F::P;
+  for (int r = 0; r < 4; r++)
+    for (int j = 0; j < 16; j++) {
+      ext[r][j] = B::to_monty(RC_RAW[r][j] % p);
+      ext[4 + r][j] = B::to_monty(RC_RAW[4 + F::ROUNDS_P + r][j] % p);
+    }
+  for (int r = 0; r < F::ROUNDS_P; r++) inte[r] = B::to_monty(RC_RAW[4 + r][0] % p);
+  // Internal diagonal (vm/src/primitives/consts.rs:110-154), canonical values.
+  uint32_t d[16];
+  if (F::ID == 0) {
+    const uint32_t k[16] = {p - 2, 1, 2, (p + 1) >> 1, 3, 4, (p - 1) >> 1, p - 3, p - 4,
+                            p - ((p - 1) >> 8), p - ((p - 1) >> 3), p - 127, (p - 1) >> 8, (p - 1) >> 3,
+                            (p - 1) >> 4, 127};
+    memcpy(d, k, sizeof d);
+  } else {
+    const uint32_t k[16] = {p - 2, 1, 2, (p + 1) >> 1, 3, 4, (p - 1) >> 1, p - 3, p - 4,
+                            p - ((p - 1) >> 8), p - ((p - 1) >> 2), p - ((p - 1) >> 3), p - 15, (p - 1) >> 8,
+                            (p - 1) >> 4, 15};
+    memcpy(d, k, sizeof d);
+  }
+  for (int j = 0; j < 16; j++) diag[j] = B::to_monty(d[j]);
+}
+
+template <class F>
+static void host_twiddles(std::vector<uint32_t>& t) {
+  using B = Fp<F>;
+  t.assign(2 * 16384, 0);
+  const uint32_t g = B::to_monty(F::GENERATOR);
+  const uint32_t w = B::pow(g, (uint64_t)(F::P - 1) >> F::TWO_ADICITY);
+  t[0] = F::ONE;
+  for (int j = 1; j < 16384; j++) t[j] = B::mul(t[j - 1], w);
+  const uint32_t w14 = B::pow(w, 1ull << 14);
+  t[16384] = F::ONE;
+  for (int j = 1; j < 16384; j++) t[16384 + j] = B::mul(t[16384 + j - 1], w14);
+}
+
+static uint32_t field_two_adicity(int field) { return field == 0 ? 24u : 27u; }
+
+}  // namespace pico
+
+// ---------------------------------------------------------------------------
+// Context
+
+pico_ctx::~pico_ctx() = default;
+
+static pico_status alloc_async(void** p, size_t bytes, cudaStream_t st) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  return cuda_status(cudaMallocAsync(p, bytes, st), "device allocation");
+}
+
+static void free_async(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
+extern "C" uint32_t pico_gpu_abi_version(void) { return PICO_GPU_ABI_VERSION; }
+extern "C" const char* pico_gpu_last_error(void) { return g_err.c_str(); }
+
+extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ctx** out) {
+  if (!out) {
+    set_error("pico_gpu_init: null output pointer");
+    return PICO_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("pico_gpu_init: no CUDA device");
+    return PICO_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("pico_gpu_init: device %d out of range (%d devices)", device, ndev);
+    return PICO_ERR_INVALID_ARG;
+  }
+  pico_status s;
+  if ((s = cuda_status(cudaSetDevice(device), "cudaSetDevice"))) return s;
+  cudaDeviceProp prop;
+  if ((s = cuda_status(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties"))) return s;
+  if (prop.major < 10) {
+    set_error("pico_gpu_init: device %d is sm_%d%d; this library is built for sm_100a", device, prop.major,
+              prop.minor);
+    return PICO_ERR_UNSUPPORTED;
+  }
+  auto ctx = std::make_unique<pico_ctx>();
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  // Keep freed memory cached in the device pool instead of returning it.
+  cudaMemPool_t pool;
+  if ((s = cuda_status(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool"))) return s;
+  uint64_t thresh = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh);
+  size_t free_b = 0, total_b = 0;
+  if ((s = cuda_status(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo"))) return s;
+  ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
+  const uint32_t ns = (cfg && cfg->n_streams) ? cfg->n_streams : 8;
+  for (uint32_t i = 0; i < ns; i++) {
+    cudaStream_t st;
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
+    ctx->streams.push_back(st);
+  }
+  // Constant tables for both fields.
+  {
+    uint32_t ext[8][16], inte[24] = {0}, diag[16];
+    host_p2_constants<KoalaBear>(ext, inte, diag);
+    if ((s = cuda_status(upload_p2_constants(0, ext, inte, KoalaBear::ROUNDS_P, diag), "constants"))) return s;
+    host_p2_constants<BabyBear>(ext, inte, diag);
+    if ((s = cuda_status(upload_p2_constants(1, ext, inte, BabyBear::ROUNDS_P, diag), "constants"))) return s;
+  }
+  for (int f = 0; f < 2; f++) {
+    std::vector<uint32_t> t;
+    if (f == 0)
+      host_twiddles<KoalaBear>(t);
+    else
+      host_twiddles<BabyBear>(t);
+    void* d = nullptr;
+    if ((s = cuda_status(cudaMalloc(&d, t.size() * 4), "twiddle tables"))) return s;
+    if ((s = cuda_status(cudaMemcpy(d, t.data(), t.size() * 4, cudaMemcpyHostToDevice), "twiddle upload")))
+      return s;
+    ctx->tw[f] = (uint32_t*)d;
+  }
+  if ((s = serving_start(ctx.get()))) return s;
+  *out = ctx.release();
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_shutdown(pico_ctx* ctx) {
+  if (!ctx) return PICO_OK;
+  cudaSetDevice(ctx->device);
+  serving_stop(ctx);
+  for (auto st : ctx->streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (int f = 0; f < 2; f++)
+    if (ctx->tw[f]) cudaFree(ctx->tw[f]);
+  delete ctx;
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_memory(pico_ctx* ctx, uint64_t* reserved, uint64_t* budget) {
+  if (!ctx) {
+    set_error("null context");
+    return PICO_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (reserved) *reserved = ctx->reserved;
+  if (budget) *budget = ctx->budget;
+  return PICO_OK;
+}
+
+namespace pico {
+
+bool try_reserve(pico_ctx* ctx, uint64_t bytes) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (ctx->reserved + bytes > ctx->budget) return false;
+  ctx->reserved += bytes;
+  return true;
+}
+void unreserve(pico_ctx* ctx, uint64_t bytes) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->reserved = bytes > ctx->reserved ? 0 : ctx->reserved - bytes;
+  ctx->cv.notify_all();
+}
+cudaStream_t pick_stream(pico_ctx* ctx) {
+  uint32_t i = ctx->next_stream.fetch_add(1) % (uint32_t)ctx->streams.size();
+  return ctx->streams[i];
+}
+TwiddleTables twiddles(pico_ctx* ctx, int field) {
+  TwiddleTables t;
+  t.lo = ctx->tw[field];
+  t.hi = ctx->tw[field] + 16384;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// Commit planning
+
+pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t log_b, uint32_t flags, bool extend,
+                        CommitPlan& plan) {
+  if (field != PICO_KOALABEAR && field != PICO_BABYBEAR) {
+    set_error("unknown field %d", field);
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (!mats || n == 0) {
+    set_error("commit: no matrices");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint32_t S = field_two_adicity(field);
+  plan = CommitPlan{};
+  plan.field = field;
+  plan.log_b = extend ? log_b : 0;
+  plan.extend = extend;
+  plan.input_device = (flags & PICO_INPUT_DEVICE) != 0;
+  plan.plain = (flags & PICO_COMMIT_PLAIN) != 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const pico_matrix& m = mats[i];
+    if (m.log_height > 30 || (extend && m.log_height + log_b > S)) {
+      set_error("commit: matrix %u height 2^%u with blowup 2^%u exceeds two-adicity %u", i, m.log_height, log_b, S);
+      return PICO_ERR_INVALID_ARG;
+    }
+    if (!m.values && m.width) {
+      set_error("commit: matrix %u has null values", i);
+      return PICO_ERR_INVALID_ARG;
+    }
+    PlannedMat pm;
+    pm.input_idx = i;
+    pm.log_n = m.log_height;
+    pm.log_N = m.log_height + plan.log_b;
+    pm.w = m.width;
+    pm.shift = m.shift;
+    pm.src = m.values;
+    plan.mats.push_back(pm);
+    plan.cells += (uint64_t)m.width << m.log_height;
+  }
+  std::stable_sort(plan.mats.begin(), plan.mats.end(),
+                   [](const PlannedMat& a, const PlannedMat& b) { return a.log_N > b.log_N; });
+  plan.log_max = plan.mats[0].log_N;
+  for (uint32_t i = 0; i < n;) {
+    uint32_t j = i;
+    while (j < n && plan.mats[j].log_N == plan.mats[i].log_N) j++;
+    if (j - i > (uint32_t)kMaxSegs) {
+      set_error("commit: %u matrices share height 2^%u (max %d)", j - i, plan.mats[i].log_N, kMaxSegs);
+      return PICO_ERR_UNSUPPORTED;
+    }
+    plan.groups.push_back({i, j});
+    i = j;
+  }
+  // Memory footprint.
+  uint64_t res = 0, scr = 0;
+  for (auto& m : plan.mats) {
+    const uint64_t cells_in = (uint64_t)m.w << m.log_n;
+    const uint64_t cells_out = (uint64_t)m.w << m.log_N;
+    if (extend) {
+      res += cells_out * 4;
+      if (!plan.input_device) scr += cells_in * 4;
+      if (m.log_n > (uint32_t)kLdeSmallMaxLog) scr += (cells_in + cells_out) * 4;
+      scr += (8192ull << plan.log_b) * 4 + 64;
+    } else if (!plan.input_device) {
+      res += cells_in * 4;
+    }
+  }
+  res += ((2ull << plan.log_max) - 1) * 32;
+  scr += 4096 + n * (sizeof(LdeMat) + 16);
+  // Work counts: one permutation per 8 absorbed elements per row of each
+  // height group, one compression per internal node, one more per injected node.
+  for (size_t gi = 0; gi < plan.groups.size(); gi++) {
+    uint64_t wsum = 0;
+    for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) {
+      wsum += plan.mats[k].w;
+      plan.lde_cells += (uint64_t)plan.mats[k].w << plan.mats[k].log_N;
+    }
+    const uint64_t rows = 1ull << plan.mats[plan.groups[gi].first].log_N;
+    const uint64_t absorb = rows * ((wsum + 7) / 8);
+    if (gi == 0)
+      plan.leaf_permutations = absorb;
+    else
+      plan.permutations += absorb + rows;
+  }
+  plan.permutations += plan.leaf_permutations + ((1ull << plan.log_max) - 1);
+  plan.bytes_resident = res;
+  plan.bytes_scratch = scr;
+  return PICO_OK;
+}
+
+// Enqueue a whole commit on `st`.  On success `c` holds the resident buffers
+// and `scratch` the buffers to free once the stream has passed this point.
+pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, pico_commit* c,
+                           std::vector<void*>& scratch, uint32_t* root_host) {
+  pico_status s;
+  const int field = plan.field;
+  const uint32_t n = (uint32_t)plan.mats.size();
+  c->ctx = ctx;
+  c->field = field;
+  c->log_max = plan.log_max;
+  c->n_mats = n;
+  c->lde.assign(n, nullptr);
+  c->log_N.assign(n, 0);
+  c->width.assign(n, 0);
+  c->owns.assign(n, false);
+  c->bytes_resident = plan.bytes_resident;
+  c->stats.cells = plan.cells;
+  c->stats.lde_cells = plan.extend ? plan.lde_cells : 0;
+  c->stats.permutations = plan.permutations;
+  c->stats.leaf_permutations = plan.leaf_permutations;
+  c->stats.lde_bytes = plan.extend ? 4 * (plan.cells + plan.lde_cells) : 0;
+  for (int e = 0; e < 5; e++)
+    if ((s = cuda_status(cudaEventCreate(&c->ev[e]), "event"))) return s;
+  if ((s = cuda_status(cudaEventRecord(c->ev[0], st), "event"))) return s;
+
+  // Device copies of the inputs (or the caller's device pointers).
+  std::vector<const uint32_t*> dev_in(n, nullptr);
+  for (uint32_t k = 0; k < n; k++) {
+    const PlannedMat& m = plan.mats[k];
+    const uint64_t bytes = ((uint64_t)m.w << m.log_n) * 4;
+    if (plan.input_device || bytes == 0) {
+      dev_in[k] = m.src;
+    } else {
+      void* d;
+      if ((s = alloc_async(&d, bytes, st))) return s;
+      if (plan.extend)
+        scratch.push_back(d);
+      else {
+        c->owns[m.input_idx] = true;
+      }
+      if ((s = cuda_status(cudaMemcpyAsync(d, m.src, bytes, cudaMemcpyHostToDevice, st), "input copy"))) return s;
+      dev_in[k] = (const uint32_t*)d;
+    }
+  }
+
+  if ((s = cuda_status(cudaEventRecord(c->ev[1], st), "event"))) return s;
+  std::vector<const uint32_t*> leaves(n, nullptr);  // what the tree hashes, per planned matrix
+  if (plan.extend) {
+    std::vector<LdeMat> hm(n);
+    const uint32_t nb = 1u << plan.log_b;
+    void* pw;  // one allocation for all (matrix, coset) power tables
+    if ((s = alloc_async(&pw, (uint64_t)n * nb * kPwWords * 4, st))) return s;
+    scratch.push_back(pw);
+    for (uint32_t k = 0; k < n; k++) {
+      const PlannedMat& m = plan.mats[k];
+      LdeMat& L = hm[k];
+      memset(&L, 0, sizeof L);
+      L.in = dev_in[k];
+      L.log_n = m.log_n;
+      L.log_b = plan.log_b;
+      L.w = m.w;
+      L.shift = m.shift % (field == 0 ? KoalaBear::P : BabyBear::P);
+      L.pw = (uint32_t*)pw + (uint64_t)k * nb * kPwWords;
+      plan_lde_tiling(L);
+      void* out;
+      if ((s = alloc_async(&out, ((uint64_t)m.w << m.log_N) * 4, st))) return s;
+      L.out = (uint32_t*)out;
+      c->lde[m.input_idx] = L.out;
+      c->owns[m.input_idx] = true;
+      c->log_N[m.input_idx] = m.log_N;
+      c->width[m.input_idx] = m.w;
+      leaves[k] = L.out;
+      if (L.log_n1) {
+        void *t1, *t2;
+        if ((s = alloc_async(&t1, ((uint64_t)m.w << m.log_n) * 4, st))) return s;
+        scratch.push_back(t1);
+        if ((s = alloc_async(&t2, ((uint64_t)m.w << m.log_N) * 4, st))) return s;
+        scratch.push_back(t2);
+        L.t1 = (uint32_t*)t1;
+        L.t2 = (uint32_t*)t2;
+      }
+    }
+    const TwiddleTables tw = twiddles(ctx, field);
+    if (plan.plain) {
+      for (uint32_t k = 0; k < n; k++)
+        if ((s = cuda_status(launch_lde(field, &hm[k], 1, tw, st, &c->stats.launches), "LDE launch"))) return s;
+    } else {
+      if ((s = cuda_status(launch_lde(field, hm.data(), n, tw, st, &c->stats.launches), "LDE launch"))) return s;
+    }
+  } else {
+    for (uint32_t k = 0; k < n; k++) {
+      const PlannedMat& m = plan.mats[k];
+      leaves[k] = dev_in[k];
+      c->lde[m.input_idx] = const_cast<uint32_t*>(dev_in[k]);
+      c->log_N[m.input_idx] = m.log_N;
+      c->width[m.input_idx] = m.w;
+    }
+  }
+
+  if ((s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) return s;
+  // Merkle tree over all (extended) matrices.
+  const uint32_t log_max = plan.log_max;
+  const uint64_t total_digests = (2ull << log_max) - 1;
+  void* layers;
+  if ((s = alloc_async(&layers, total_digests * 32, st))) return s;
+  c->layers = (uint32_t*)layers;
+  auto make_group = [&](uint32_t gi, RowGroup& g) {
+    memset(&g, 0, sizeof g);
+    const auto& gr = plan.groups[gi];
+    g.n_segs = gr.second - gr.first;
+    for (uint32_t k = gr.first; k < gr.second; k++) {
+      g.segs[k - gr.first].ptr = leaves[k];
+      g.segs[k - gr.first].width = plan.mats[k].w;
+      g.total_width += plan.mats[k].w;
+    }
+  };
+  RowGroup g0;
+  make_group(0, g0);
+  uint32_t* layer = c->layers;
+  if ((s = cuda_status(launch_hash_rows(field, g0, 1ull << log_max, layer, st), "leaf hashing"))) return s;
+  c->stats.launches += 1;
+  if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;
+  uint32_t next_group = 1;
+  for (uint32_t lvl = 1; lvl <= log_max; lvl++) {
+    const uint64_t len = 1ull << (log_max - lvl);
+    uint32_t* next = layer + (2 * len) * 8;
+    RowGroup gi;
+    const RowGroup* inj = nullptr;
+    if (next_group < plan.groups.size() && plan.mats[plan.groups[next_group].first].log_N == log_max - lvl) {
+      make_group(next_group, gi);
+      inj = &gi;
+      next_group++;
+    }
+    if ((s = cuda_status(launch_compress(field, layer, next, len, inj, st), "compression"))) return s;
+    c->stats.launches += 1;
+    layer = next;
+  }
+  if ((s = cuda_status(cudaEventRecord(c->ev[4], st), "event"))) return s;
+  if (root_host)
+    if ((s = cuda_status(cudaMemcpyAsync(root_host, layer, 32, cudaMemcpyDeviceToHost, st), "root copy"))) return s;
+  return PICO_OK;
+}
+
+// Fill c->stats timings from its events (blocks until the commit finished).
+pico_status finish_stats(pico_commit* c) {
+  if (!c->ev[4]) return PICO_OK;
+  pico_status s;
+  if ((s = cuda_status(cudaEventSynchronize(c->ev[4]), "commit events"))) return s;
+  float t[4];
+  for (int i = 0; i < 4; i++)
+    if ((s = cuda_status(cudaEventElapsedTime(&t[i], c->ev[i], c->ev[i + 1]), "event timing"))) return s;
+  c->stats.h2d_ms = t[0];
+  c->stats.lde_ms = t[1];
+  c->stats.leaves_ms = t[2];
+  c->stats.tree_ms = t[3];
+  c->stats.total_ms = (double)t[0] + t[1] + t[2] + t[3];
+  for (int e = 0; e < 5; e++) {
+    cudaEventDestroy(c->ev[e]);
+    c->ev[e] = nullptr;
+  }
+  return PICO_OK;
+}
+
+void free_commit_buffers(pico_commit* c, cudaStream_t st) {
+  for (uint32_t i = 0; i < c->lde.size(); i++)
+    if (c->owns[i]) free_async(c->lde[i], st);
+  free_async(c->layers, st);
+  c->lde.clear();
+  c->layers = nullptr;
+}
+
+}  // namespace pico
+
+pico_commit::~pico_commit() {
+  for (int e = 0; e < 5; e++)
+    if (ev[e]) cudaEventDestroy(ev[e]);
+}
+
+static thread_local pico_commit_stats g_last_stats{};
+
+// ---------------------------------------------------------------------------
+// Synchronous commit
+
+static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_matrix* mats, uint32_t n_mats,
+                                 uint32_t log_blowup, uint32_t flags, pico_commit** out, uint32_t root[8],
+                                 bool extend) {
+  if (!ctx || !root) {
+    set_error("commit: null context or root");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (out) *out = nullptr;
+  pico_status s;
+  CommitPlan plan;
+  if ((s = plan_commit(field, mats, n_mats, log_blowup, flags, extend, plan))) return s;
+  const uint64_t need = plan.bytes_resident + plan.bytes_scratch;
+  if (!try_reserve(ctx, need)) {
+    set_error("commit: needs %llu bytes, HBM budget has %llu of %llu reserved", (unsigned long long)need,
+              (unsigned long long)ctx->reserved, (unsigned long long)ctx->budget);
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  auto c = std::make_unique<pico_commit>();
+  std::vector<void*> scratch;
+  uint32_t root_h[8];
+  s = enqueue_commit(ctx, plan, st, c.get(), scratch, root_h);
+  for (void* p : scratch) cudaFreeAsync(p, st);
+  pico_status s2 = cuda_status(cudaStreamSynchronize(st), "commit");
+  if (!s) s = s2;
+  unreserve(ctx, plan.bytes_scratch);
+  if (s) {
+    free_commit_buffers(c.get(), st);
+    cudaStreamSynchronize(st);
+    unreserve(ctx, plan.bytes_resident);
+    return s;
+  }
+  memcpy(c->root, root_h, 32);
+  memcpy(root, root_h, 32);
+  finish_stats(c.get());
+  g_last_stats = c->stats;
+  if (out) {
+    *out = c.release();
+  } else {
+    free_commit_buffers(c.get(), st);
+    cudaStreamSynchronize(st);
+    unreserve(ctx, plan.bytes_resident);
+  }
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_commit(pico_ctx* ctx, pico_field field, const pico_matrix* mats, uint32_t n_mats,
+                                       uint32_t log_blowup, uint32_t flags, pico_commit** out, uint32_t root[8]) {
+  return commit_common(ctx, field, mats, n_mats, log_blowup, flags, out, root, true);
+}
+
+extern "C" pico_status pico_gpu_mmcs_commit(pico_ctx* ctx, pico_field field, const pico_matrix* mats,
+                                            uint32_t n_mats, uint32_t flags, pico_commit** out, uint32_t root[8]) {
+  return commit_common(ctx, field, mats, n_mats, 0, flags, out, root, false);
+}
+
+extern "C" pico_status pico_gpu_commit_stats(const pico_commit* c, pico_commit_stats* out) {
+  if (!c || !out) {
+    set_error("commit_stats: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  pico_status s = finish_stats(const_cast<pico_commit*>(c));
+  if (s) return s;
+  *out = c->stats;
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_last_commit_stats(pico_commit_stats* out) {
+  if (!out) {
+    set_error("last_commit_stats: null output");
+    return PICO_ERR_INVALID_ARG;
+  }
+  *out = g_last_stats;
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_release(pico_ctx* ctx, pico_commit* c) {
+  if (!c) return PICO_OK;
+  if (!ctx || c->ctx != ctx) {
+    set_error("release: commit belongs to another context");
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  free_commit_buffers(c, st);
+  pico_status s = cuda_status(cudaStreamSynchronize(st), "release");
+  unreserve(ctx, c->bytes_resident);
+  delete c;
+  return s;
+}
+
+extern "C" pico_status pico_gpu_lde_shape(const pico_commit* c, uint32_t mat_idx, uint32_t* log_height,
+                                          uint32_t* width) {
+  if (!c || mat_idx >= c->n_mats) {
+    set_error("lde_shape: bad commit or index");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (log_height) *log_height = c->log_N[mat_idx];
+  if (width) *width = c->width[mat_idx];
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_lde_rows(pico_ctx* ctx, const pico_commit* c, uint32_t mat_idx, uint64_t row_begin,
+                                         uint64_t row_end, uint32_t* out, uint32_t flags) {
+  if (!ctx || !c || !out || mat_idx >= c->n_mats) {
+    set_error("lde_rows: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint64_t N = 1ull << c->log_N[mat_idx];
+  if (row_begin > row_end || row_end > N) {
+    set_error("lde_rows: rows [%llu, %llu) outside height %llu", (unsigned long long)row_begin,
+              (unsigned long long)row_end, (unsigned long long)N);
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  const uint64_t w = c->width[mat_idx];
+  const size_t bytes = (row_end - row_begin) * w * 4;
+  if (!bytes) return PICO_OK;
+  cudaStream_t st = pick_stream(ctx);
+  pico_status s = cuda_status(cudaMemcpyAsync(out, c->lde[mat_idx] + row_begin * w, bytes,
+                                              (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice
+                                                                           : cudaMemcpyDeviceToHost,
+                                              st),
+                              "lde_rows copy");
+  if (s) return s;
+  return cuda_status(cudaStreamSynchronize(st), "lde_rows");
+}
+
+extern "C" pico_status pico_gpu_digest_layer(pico_ctx* ctx, const pico_commit* c, uint32_t level, uint32_t* out,
+                                             uint32_t flags) {
+  if (!ctx || !c || !out || level > c->log_max) {
+    set_error("digest_layer: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  uint64_t off = 0;
+  for (uint32_t l = 0; l < level; l++) off += 1ull << (c->log_max - l);
+  const size_t bytes = (1ull << (c->log_max - level)) * 32;
+  cudaStream_t st = pick_stream(ctx);
+  pico_status s = cuda_status(
+      cudaMemcpyAsync(out, c->layers + off * 8, bytes,
+                      (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st),
+      "digest copy");
+  if (s) return s;
+  return cuda_status(cudaStreamSynchronize(st), "digest_layer");
+}
+
+extern "C" pico_status pico_gpu_open_batch(pico_ctx* ctx, const pico_commit* c, uint64_t index, uint32_t* rows_out,
+                                           uint32_t* path_out) {
+  if (!ctx || !c || index >= (1ull << c->log_max)) {
+    set_error("open_batch: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  pico_status s;
+  if (rows_out) {
+    uint64_t off = 0;
+    for (uint32_t i = 0; i < c->n_mats; i++) {
+      const uint64_t r = index >> (c->log_max - c->log_N[i]);
+      const uint64_t w = c->width[i];
+      if (w) {
+        s = cuda_status(cudaMemcpyAsync(rows_out + off, c->lde[i] + r * w, w * 4, cudaMemcpyDeviceToHost, st),
+                        "open_batch rows");
+        if (s) return s;
+      }
+      off += w;
+    }
+  }
+  if (path_out) {
+    uint64_t off = 0;
+    for (uint32_t l = 0; l < c->log_max; l++) {
+      const uint64_t sib = (index >> l) ^ 1ull;
+      s = cuda_status(cudaMemcpyAsync(path_out + 8 * l, c->layers + (off + sib) * 8, 32, cudaMemcpyDeviceToHost, st),
+                      "open_batch path");
+      if (s) return s;
+      off += 1ull << (c->log_max - l);
+    }
+  }
+  return cuda_status(cudaStreamSynchronize(st), "open_batch");
+}
+
+// ---------------------------------------------------------------------------
+// Dft / permutation entry points
+
+extern "C" pico_status pico_gpu_coset_lde_batch(pico_ctx* ctx, pico_field field, const uint32_t* in, uint32_t log_n,
+                                                uint32_t width, uint32_t log_blowup, uint32_t shift, uint32_t* out,
+                                                uint32_t flags) {
+  if (!ctx || !in || !out || (field != PICO_KOALABEAR && field != PICO_BABYBEAR)) {
+    set_error("coset_lde_batch: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (log_n + log_blowup > field_two_adicity(field)) {
+    set_error("coset_lde_batch: 2^%u rows with blowup 2^%u exceeds the two-adicity", log_n, log_blowup);
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (flags & PICO_LDE_NATURAL_ORDER) {
+    set_error("coset_lde_batch: natural row order is not implemented; the committed order is bit-reversed");
+    return PICO_ERR_UNSUPPORTED;
+  }
+  pico_matrix m{in, log_n, width, shift, 0};
+  CommitPlan plan;
+  pico_status s;
+  if ((s = plan_commit(field, &m, 1, log_blowup, flags, true, plan))) return s;
+  const uint64_t out_bytes = ((uint64_t)width << (log_n + log_blowup)) * 4;
+  const uint64_t need = plan.bytes_scratch + out_bytes;
+  if (!try_reserve(ctx, need)) {
+    set_error("coset_lde_batch: HBM budget exceeded");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  std::vector<void*> scratch;
+  // Reuse the commit planner's LDE path without the tree: build the LdeMat directly.
+  LdeMat L;
+  memset(&L, 0, sizeof L);
+  L.log_n = log_n;
+  L.log_b = log_blowup;
+  L.w = width;
+  plan_lde_tiling(L);
+  const uint64_t in_bytes = ((uint64_t)width << log_n) * 4;
+  auto run = [&]() -> pico_status {
+    void* p;
+    if (flags & PICO_INPUT_DEVICE) {
+      L.in = in;
+    } else {
+      if ((s = alloc_async(&p, in_bytes, st))) return s;
+      scratch.push_back(p);
+      if ((s = cuda_status(cudaMemcpyAsync(p, in, in_bytes, cudaMemcpyHostToDevice, st), "input copy"))) return s;
+      L.in = (const uint32_t*)p;
+    }
+    if (flags & PICO_OUTPUT_DEVICE) {
+      L.out = out;
+    } else {
+      if ((s = alloc_async(&p, out_bytes, st))) return s;
+      scratch.push_back(p);
+      L.out = (uint32_t*)p;
+    }
+    if (L.log_n1) {
+      if ((s = alloc_async(&p, in_bytes, st))) return s;
+      scratch.push_back(p);
+      L.t1 = (uint32_t*)p;
+      if ((s = alloc_async(&p, out_bytes, st))) return s;
+      scratch.push_back(p);
+      L.t2 = (uint32_t*)p;
+    }
+    const uint32_t nb = 1u << log_blowup;
+    if ((s = alloc_async(&p, (uint64_t)nb * kPwWords * 4, st))) return s;
+    scratch.push_back(p);
+    L.pw = (uint32_t*)p;
+    L.shift = shift % (field == 0 ? KoalaBear::P : BabyBear::P);
+    if ((s = cuda_status(launch_lde(field, &L, 1, twiddles(ctx, field), st), "LDE"))) return s;
+    if (!(flags & PICO_OUTPUT_DEVICE))
+      if ((s = cuda_status(cudaMemcpyAsync(out, L.out, out_bytes, cudaMemcpyDeviceToHost, st), "output copy")))
+        return s;
+    return PICO_OK;
+  };
+  s = run();
+  for (void* p : scratch) cudaFreeAsync(p, st);
+  pico_status s2 = cuda_status(cudaStreamSynchronize(st), "coset_lde_batch");
+  unreserve(ctx, need);
+  return s ? s : s2;
+}
+
+extern "C" pico_status pico_gpu_poseidon2_permute(pico_ctx* ctx, pico_field field, uint32_t* states, uint64_t n,
+                                                  uint32_t flags) {
+  if (!ctx || (!states && n) || (field != PICO_KOALABEAR && field != PICO_BABYBEAR)) {
+    set_error("poseidon2_permute: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (!n) return PICO_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  pico_status s;
+  const uint64_t bytes = n * 64;
+  if (flags & PICO_INPUT_DEVICE) {
+    if ((s = cuda_status(launch_permute(field, states, n, st), "permute"))) return s;
+    return cuda_status(cudaStreamSynchronize(st), "permute");
+  }
+  if (!try_reserve(ctx, bytes)) {
+    set_error("poseidon2_permute: HBM budget exceeded");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  void* d;
+  s = alloc_async(&d, bytes, st);
+  if (!s) s = cuda_status(cudaMemcpyAsync(d, states, bytes, cudaMemcpyHostToDevice, st), "copy in");
+  if (!s) s = cuda_status(launch_permute(field, (uint32_t*)d, n, st), "permute");
+  if (!s) s = cuda_status(cudaMemcpyAsync(states, d, bytes, cudaMemcpyDeviceToHost, st), "copy out");
+  free_async(d, st);
+  pico_status s2 = cuda_status(cudaStreamSynchronize(st), "permute");
+  unreserve(ctx, bytes);
+  return s ? s : s2;
+}

@@ -1,0 +1,234 @@
+// FRI commit phase on device-resident codewords (the loop inside
+// TwoAdicFriPcs::open, prover.rs:589; mirrored by the verifier's
+// verify_shape_and_sample_challenges, vm/src/compiler/recursion/circuit/fri.rs:45-52).
+//
+// Every round runs on one stream with no host round trip: leaf hashing of the
+// codeword viewed as a (len/2) x 8 base matrix (ExtensionMmcs flattening, one
+// permutation per leaf), compression up to the root, the duplex challenger
+// observing the root and sampling beta on the device, then the fold.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+#include "runtime.h"
+
+using namespace pico;
+
+static pico_status fri_alloc(void** p, size_t bytes, cudaStream_t st) {
+  return cuda_status(cudaMallocAsync(p, bytes ? bytes : 16, st), "device allocation");
+}
+
+extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field, const uint32_t* codeword,
+                                                 uint32_t log_n, uint32_t log_blowup, uint32_t log_final_len,
+                                                 const uint32_t* betas_in, pico_challenger* ch, uint32_t flags,
+                                                 uint32_t* roots, uint32_t* betas, uint32_t* final_out,
+                                                 uint32_t* n_rounds, pico_fri** out) {
+  if (out) *out = nullptr;
+  if (!ctx || !codeword || (field != PICO_KOALABEAR && field != PICO_BABYBEAR)) {
+    set_error("fri_commit_phase: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint32_t S = field == PICO_KOALABEAR ? 24u : 27u;
+  const uint32_t log_stop = log_blowup + log_final_len;
+  if (log_n > S || log_n < log_stop || log_n < 1) {
+    set_error("fri_commit_phase: codeword 2^%u vs stop length 2^%u (two-adicity %u)", log_n, log_stop, S);
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (!betas_in && !ch) {
+    set_error("fri_commit_phase: need a challenger state or explicit betas");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint32_t R = log_n - log_stop;
+  // Footprint: all codewords, all trees, small buffers.
+  uint64_t resident = 0;
+  for (uint32_t r = 0; r <= R; r++) resident += (16ull << (log_n - r));
+  for (uint32_t r = 0; r < R; r++) resident += ((2ull << (log_n - r - 1)) - 1) * 32;
+  const uint64_t small = 4096 + 16ull * (R + 1) + (16ull << log_final_len);
+  if (!try_reserve(ctx, resident + small)) {
+    set_error("fri_commit_phase: HBM budget exceeded");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  auto f = std::make_unique<pico_fri>();
+  f->ctx = ctx;
+  f->field = field;
+  f->log_n = log_n;
+  f->rounds = R;
+  f->bytes_resident = resident;
+  std::vector<void*> scratch;
+  std::vector<uint32_t> final_cw(4u << log_stop);
+  uint32_t err_flag = 0;
+  const TwiddleTables tw = twiddles(ctx, field);
+
+  auto run = [&]() -> pico_status {
+    pico_status s;
+    void* p;
+    for (uint32_t r = 0; r <= R; r++) {
+      if ((s = fri_alloc(&p, 16ull << (log_n - r), st))) return s;
+      f->codewords.push_back((uint32_t*)p);
+    }
+    for (uint32_t r = 0; r < R; r++) {
+      if ((s = fri_alloc(&p, ((2ull << (log_n - r - 1)) - 1) * 32, st))) return s;
+      f->trees.push_back((uint32_t*)p);
+    }
+    if ((s = cuda_status(cudaMemcpyAsync(f->codewords[0], codeword, 16ull << log_n,
+                                         (flags & PICO_INPUT_DEVICE) ? cudaMemcpyDeviceToDevice
+                                                                     : cudaMemcpyHostToDevice,
+                                         st),
+                         "codeword copy")))
+      return s;
+    uint32_t *d_betas, *d_err, *d_final;
+    DevChallenger* d_ch = nullptr;
+    if ((s = fri_alloc(&p, 16ull * (R + 1), st))) return s;
+    scratch.push_back(p);
+    d_betas = (uint32_t*)p;
+    if ((s = fri_alloc(&p, 16, st))) return s;
+    scratch.push_back(p);
+    d_err = (uint32_t*)p;
+    if ((s = fri_alloc(&p, 16ull << log_final_len, st))) return s;
+    scratch.push_back(p);
+    d_final = (uint32_t*)p;
+    if ((s = cuda_status(cudaMemsetAsync(d_err, 0, 4, st), "memset"))) return s;
+    if (betas_in) {
+      if ((s = cuda_status(cudaMemcpyAsync(d_betas, betas_in, 16ull * R, cudaMemcpyHostToDevice, st), "betas")))
+        return s;
+    }
+    if (ch) {
+      static_assert(sizeof(DevChallenger) == sizeof(pico_challenger), "challenger layout");
+      if ((s = fri_alloc(&p, sizeof(DevChallenger), st))) return s;
+      scratch.push_back(p);
+      d_ch = (DevChallenger*)p;
+      if ((s = cuda_status(cudaMemcpyAsync(d_ch, ch, sizeof *ch, cudaMemcpyHostToDevice, st), "challenger")))
+        return s;
+    }
+    for (uint32_t r = 0; r < R; r++) {
+      const uint32_t L = log_n - r;            // codeword length 2^L
+      const uint64_t leaves = 1ull << (L - 1);  // rows of the (len/2) x 8 matrix
+      RowGroup g;
+      memset(&g, 0, sizeof g);
+      g.n_segs = 1;
+      g.total_width = 8;
+      g.segs[0].ptr = f->codewords[r];
+      g.segs[0].width = 8;
+      uint32_t* layer = f->trees[r];
+      if ((s = cuda_status(launch_hash_rows(field, g, leaves, layer, st), "FRI leaf hashing"))) return s;
+      for (uint32_t lvl = 1; lvl < L; lvl++) {
+        const uint64_t len = leaves >> lvl;
+        uint32_t* next = layer + 2 * len * 8;
+        if ((s = cuda_status(launch_compress(field, layer, next, len, nullptr, st), "FRI compression"))) return s;
+        layer = next;
+      }
+      // layer now points at the root
+      if (!betas_in)
+        if ((s = cuda_status(launch_challenger_round(field, d_ch, layer, d_betas + 4 * r, st), "challenger")))
+          return s;
+      if ((s = cuda_status(launch_fri_fold_tw(field, f->codewords[r], L, d_betas + 4 * r, tw, f->codewords[r + 1], st),
+                           "fold")))
+        return s;
+    }
+    // Read-backs are queued after the whole loop: a copy into pageable host
+    // memory blocks the calling thread until the stream reaches it.
+    uint32_t* last = f->codewords[R];
+    if (log_final_len == 0) {
+      if (!betas_in)
+        if ((s = cuda_status(launch_challenger_observe(field, d_ch, last, 4, st), "observe final"))) return s;
+    } else {
+      if ((s = cuda_status(launch_fri_final_poly(field, last, log_stop, log_final_len, tw, d_final, d_err, st),
+                           "final polynomial")))
+        return s;
+      if (!betas_in)
+        if ((s = cuda_status(launch_challenger_observe(field, d_ch, d_final, 4u << log_final_len, st),
+                             "observe final")))
+          return s;
+      if (final_out)
+        if ((s = cuda_status(cudaMemcpyAsync(final_out, d_final, 16ull << log_final_len, cudaMemcpyDeviceToHost, st),
+                             "final copy")))
+          return s;
+    }
+    if ((s = cuda_status(cudaMemcpyAsync(final_cw.data(), last, 16ull << log_stop, cudaMemcpyDeviceToHost, st),
+                         "final codeword")))
+      return s;
+    if ((s = cuda_status(cudaMemcpyAsync(&err_flag, d_err, 4, cudaMemcpyDeviceToHost, st), "flag"))) return s;
+    if (roots)
+      for (uint32_t r = 0; r < R; r++) {
+        // the root is the last digest of round r's tree
+        const uint64_t leaves = 1ull << (log_n - r - 1);
+        if ((s = cuda_status(cudaMemcpyAsync(roots + 8 * r, f->trees[r] + (2 * leaves - 2) * 8, 32,
+                                             cudaMemcpyDeviceToHost, st),
+                             "root copy")))
+          return s;
+      }
+    if (betas && R)
+      if ((s = cuda_status(cudaMemcpyAsync(betas, d_betas, 16ull * R, cudaMemcpyDeviceToHost, st), "betas copy")))
+        return s;
+    if (ch && !betas_in)
+      if ((s = cuda_status(cudaMemcpyAsync(ch, d_ch, sizeof *ch, cudaMemcpyDeviceToHost, st), "challenger copy")))
+        return s;
+    return PICO_OK;
+  };
+  pico_status s = run();
+  for (void* p : scratch) cudaFreeAsync(p, st);
+  pico_status s2 = cuda_status(cudaStreamSynchronize(st), "fri_commit_phase");
+  if (!s) s = s2;
+  unreserve(ctx, small);
+  if (!s && log_final_len == 0) {
+    // Plonky3 asserts the remaining 2^b evaluations of the constant polynomial agree.
+    for (size_t i = 1; i < (size_t)1 << log_stop; i++)
+      if (memcmp(&final_cw[4 * i], &final_cw[0], 16) != 0) {
+        set_error("fri_commit_phase: final codeword is not constant (input is not of low degree)");
+        s = PICO_ERR_INVALID_ARG;
+        break;
+      }
+    if (!s && final_out) memcpy(final_out, final_cw.data(), 16);
+  }
+  if (!s && err_flag) {
+    set_error("fri_commit_phase: final polynomial has more than 2^%u coefficients", log_final_len);
+    s = PICO_ERR_INVALID_ARG;
+  }
+  if (!s && n_rounds) *n_rounds = R;
+  if (s || !out) {
+    for (auto p : f->codewords) cudaFreeAsync(p, st);
+    for (auto p : f->trees) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    unreserve(ctx, resident);
+    return s;
+  }
+  *out = f.release();
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_fri_release(pico_ctx* ctx, pico_fri* f) {
+  if (!f) return PICO_OK;
+  if (!ctx || f->ctx != ctx) {
+    set_error("fri_release: handle belongs to another context");
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  for (auto p : f->codewords) cudaFreeAsync(p, st);
+  for (auto p : f->trees) cudaFreeAsync(p, st);
+  pico_status s = cuda_status(cudaStreamSynchronize(st), "fri_release");
+  unreserve(ctx, f->bytes_resident);
+  delete f;
+  return s;
+}
+
+extern "C" pico_status pico_gpu_fri_layer(pico_ctx* ctx, const pico_fri* f, uint32_t round, uint32_t* out,
+                                          uint32_t flags) {
+  if (!ctx || !f || !out || round > f->rounds) {
+    set_error("fri_layer: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = pick_stream(ctx);
+  pico_status s = cuda_status(cudaMemcpyAsync(out, f->codewords[round], 16ull << (f->log_n - round),
+                                              (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice
+                                                                           : cudaMemcpyDeviceToHost,
+                                              st),
+                              "fri_layer copy");
+  if (s) return s;
+  return cuda_status(cudaStreamSynchronize(st), "fri_layer");
+}

@@ -1,0 +1,97 @@
+// Internal host-side interface between the C-ABI runtime (api.cu) and the
+// kernel translation units.  Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace pico {
+
+constexpr int kMaxSegs = 64;  // matrices concatenated into one Merkle row
+
+// One matrix segment of a concatenated Merkle row: `rows` x `width`,
+// row-major, rows at ptr + r * width.
+struct RowSeg {
+  const uint32_t* ptr;
+  uint32_t width;
+  uint32_t pad;
+};
+
+// Rows of all matrices of one height, concatenated in commit order (the
+// MerkleTreeMmcs leaf / injection input, fri.rs:389-436).
+struct RowGroup {
+  uint32_t n_segs;
+  uint32_t total_width;
+  RowSeg segs[kMaxSegs];
+};
+
+// --- Poseidon2 / Merkle kernels (p2_kernels.cu) -------------------------
+cudaError_t upload_p2_constants(int field, const uint32_t ext[8][16], const uint32_t* inte, int rounds_p,
+                                const uint32_t diag[16]);
+cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st);
+cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st);
+// next[i] = compress(prev[2i], prev[2i+1]); if inject != null:
+// next[i] = compress(next[i], hash(inject rows i)).
+cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,
+                            const RowGroup* inject, cudaStream_t st);
+
+// --- FRI kernels (p2_kernels.cu) ----------------------------------------
+// Device-side duplex challenger state, Monty form.
+struct DevChallenger {
+  uint32_t sponge[16];
+  uint32_t in_buf[8];
+  uint32_t in_len;
+  uint32_t out_buf[8];
+  uint32_t out_len;
+};
+// Per-field twiddle tables: lo[j] = w^j, hi[j] = w^(j * 2^14), w of order 2^S.
+struct TwiddleTables {
+  const uint32_t* lo;
+  const uint32_t* hi;
+};
+// Fold one codeword of 2^log_len EF4 elements to half length with the EF4
+// challenge at beta (device, 4 words).
+cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
+                               TwiddleTables tw, uint32_t* out, cudaStream_t st);
+// Coefficients of the final polynomial (2^log_keep x 4 words) from the last
+// codeword of 2^log_len EF4 elements; *err set if higher coefficients are nonzero.
+cudaError_t launch_fri_final_poly(int field, const uint32_t* cw, uint32_t log_len, uint32_t log_keep,
+                                  TwiddleTables tw, uint32_t* coeffs, uint32_t* err, cudaStream_t st);
+// Observe an 8-element root, then sample 4 elements into beta_out (EF4).
+cudaError_t launch_challenger_round(int field, DevChallenger* ch, const uint32_t* root, uint32_t* beta_out,
+                                    cudaStream_t st);
+// Observe n elements at vals.
+cudaError_t launch_challenger_observe(int field, DevChallenger* ch, const uint32_t* vals, uint32_t n,
+                                      cudaStream_t st);
+
+// --- LDE kernels (ntt_kernels.cu) ----------------------------------------
+struct LdeMat {
+  const uint32_t* in;  // n x w evaluations
+  uint32_t* out;       // N x w, bit-reversed rows
+  uint32_t* t1;        // n x w scratch (three-pass form only)
+  uint32_t* t2;        // N x w scratch (three-pass form only)
+  uint32_t* pw;        // 2^b tables of 8192 words: g_cb^i / n, two-level
+  uint32_t log_n, log_b, w;
+  uint32_t ws, J;          // column-tile width and adjacent sub-transforms per tile
+  uint32_t log_n1, log_n2; // three-pass split n = n1 * n2 (0 for the one-pass form)
+  uint32_t n_ct;           // number of column tiles
+  uint32_t shift;          // coset shift, Monty form
+};
+constexpr int kLdeSmallMaxLog = 11;  // one-pass form handles n <= 2^11
+constexpr int kLdeBatch = 32;        // matrices per launch (descriptors travel as kernel parameters)
+struct LdeBatch {
+  uint32_t n;
+  uint32_t pad;
+  LdeMat m[kLdeBatch];
+};
+constexpr uint32_t kPwWords = 8192;  // words per (matrix, coset) power table
+
+// Power tables then LDE kernels for `n` matrices (host descriptors, any
+// count; launched in batches of kLdeBatch).  *launches counts kernels.
+cudaError_t launch_lde(int field, const LdeMat* mats, uint32_t n, TwiddleTables tw, cudaStream_t st,
+                       uint64_t* launches = nullptr);
+
+// Choose tiling for one matrix (fills ws, J, log_n1, log_n2, n_ct).
+void plan_lde_tiling(LdeMat& m);
+
+}  // namespace pico

@@ -1,0 +1,293 @@
+// Poseidon2 kernels: batch permutation, Merkle row hashing (PaddingFreeSponge
+// rate 8, overwrite mode), 2-to-1 compression with mixed-height injection,
+// FRI fold, and the device-side duplex challenger.
+#include <cuda_runtime.h>
+
+#include "field.cuh"
+#include "internal.h"
+#include "poseidon2.cuh"
+
+namespace pico {
+
+cudaError_t upload_p2_constants(int field, const uint32_t ext[8][16], const uint32_t* inte, int rounds_p,
+                                const uint32_t diag[16]) {
+  P2Constants h{};
+  for (int r = 0; r < 8; r++)
+    for (int j = 0; j < 16; j++) h.ext[r][j] = ext[r][j];
+  for (int r = 0; r < rounds_p && r < 24; r++) h.inte[r] = inte[r];
+  for (int j = 0; j < 16; j++) h.diag[j] = diag[j];
+  return cudaMemcpyToSymbol(c_p2, &h, sizeof h, sizeof(P2Constants) * (field ? 1 : 0));
+}
+
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void k_permute(uint32_t* states, uint64_t n) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t s[16];
+  uint4* p = reinterpret_cast<uint4*>(states + 16 * i);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint4 v = p[k];
+    s[4 * k] = v.x;
+    s[4 * k + 1] = v.y;
+    s[4 * k + 2] = v.z;
+    s[4 * k + 3] = v.w;
+  }
+  p2_permute<F>(s);
+#pragma unroll
+  for (int k = 0; k < 4; k++) p[k] = make_uint4(s[4 * k], s[4 * k + 1], s[4 * k + 2], s[4 * k + 3]);
+}
+
+// Absorb row r of the concatenated group into a zeroed sponge state
+// (PaddingFreeSponge<_,16,8,8>: overwrite s[0..k) with each chunk of up to 8
+// elements, permute after each chunk; hash.rs:40-52).
+template <class F>
+__device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t s[16]) {
+  const uint32_t W = g.total_width;
+  uint32_t seg = 0, col = 0;
+  uint32_t segw = g.segs[0].width;
+  const uint32_t* rowp = g.segs[0].ptr + r * segw;
+  for (uint32_t base = 0; base < W; base += 8) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      if (base + j < W) {
+        while (col == segw) {
+          seg++;
+          col = 0;
+          segw = g.segs[seg].width;
+          rowp = g.segs[seg].ptr + r * segw;
+        }
+        s[j] = __ldg(rowp + col);
+        col++;
+      }
+    }
+    p2_permute<F>(s);
+  }
+}
+
+__device__ __forceinline__ void store_digest(uint32_t* out, const uint32_t s[16]) {
+  uint4* o = reinterpret_cast<uint4*>(out);
+  o[0] = make_uint4(s[0], s[1], s[2], s[3]);
+  o[1] = make_uint4(s[4], s[5], s[6], s[7]);
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k_hash_rows(const __grid_constant__ RowGroup g, uint64_t rows, uint32_t* out) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = 0;
+  hash_row<F>(g, r, s);
+  store_digest(out + 8 * r, s);
+}
+
+template <class F>
+__global__ void __launch_bounds__(256)
+    k_compress(const uint32_t* prev, uint32_t* next, uint64_t n, const __grid_constant__ RowGroup g) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t s[16];
+  const uint4* p = reinterpret_cast<const uint4*>(prev + 16 * i);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint4 v = __ldg(p + k);
+    s[4 * k] = v.x;
+    s[4 * k + 1] = v.y;
+    s[4 * k + 2] = v.z;
+    s[4 * k + 3] = v.w;
+  }
+  p2_permute<F>(s);
+  if (g.n_segs) {
+    uint32_t h[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) h[k] = 0;
+    hash_row<F>(g, i, h);
+#pragma unroll
+    for (int k = 0; k < 8; k++) s[8 + k] = h[k];
+    p2_permute<F>(s);
+  }
+  store_digest(next + 8 * i, s);
+}
+
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
+
+cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  if (field == 0)
+    k_permute<KoalaBear><<<blocks_for(n, 256), 256, 0, st>>>(states, n);
+  else
+    k_permute<BabyBear><<<blocks_for(n, 256), 256, 0, st>>>(states, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st) {
+  if (rows == 0) return cudaSuccess;
+  if (field == 0)
+    k_hash_rows<KoalaBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, out);
+  else
+    k_hash_rows<BabyBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,
+                            const RowGroup* inject, cudaStream_t st) {
+  if (n_next == 0) return cudaSuccess;
+  RowGroup none{};
+  const RowGroup& g = inject ? *inject : none;
+  if (field == 0)
+    k_compress<KoalaBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, g);
+  else
+    k_compress<BabyBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, g);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FRI fold (TwoAdicFriGenericConfig::fold_matrix, mirrored by the verifier at
+// vm/src/compiler/recursion/circuit/fri.rs:345-377): row r of the (len/2) x 2
+// matrix (lo, hi) folds to
+//   (lo + hi)/2 + (beta/2) * g_inv^rev(r) * (lo - hi),
+// g = two_adic_generator(log len), rev over log(len/2) bits.
+template <class F>
+__global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t* beta, TwiddleTables tw,
+                           uint32_t* out) {
+  using B = Fp<F>;
+  using E = Ef<F>;
+  const uint64_t h = 1ull << (log_len - 1);
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= h) return;
+  Ext4 hb;
+#pragma unroll
+  for (int i = 0; i < 4; i++) hb.c[i] = B::half(__ldg(beta + i));
+  // g_inv^rev(r) = w_max^(-(rev(r) << (S - log_len)))
+  const uint32_t mask = (1u << F::TWO_ADICITY) - 1u;
+  uint32_t e = (uint32_t)bitrev64(r, (int)log_len - 1) << (F::TWO_ADICITY - log_len);
+  e = (0u - e) & mask;
+  uint32_t t = B::mul(__ldg(tw.hi + (e >> 14)), __ldg(tw.lo + (e & 0x3fffu)));
+  const uint4 lo4 = __ldg(reinterpret_cast<const uint4*>(cw) + 2 * r);
+  const uint4 hi4 = __ldg(reinterpret_cast<const uint4*>(cw) + 2 * r + 1);
+  Ext4 lo{{lo4.x, lo4.y, lo4.z, lo4.w}}, hi{{hi4.x, hi4.y, hi4.z, hi4.w}};
+  Ext4 sum = E::add(lo, hi), dif = E::sub(lo, hi);
+  Ext4 res;
+  Ext4 pd = E::mul(hb, E::scale(dif, t));
+#pragma unroll
+  for (int i = 0; i < 4; i++) res.c[i] = B::add(B::half(sum.c[i]), pd.c[i]);
+  reinterpret_cast<uint4*>(out)[r] = make_uint4(res.c[0], res.c[1], res.c[2], res.c[3]);
+}
+
+cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
+                               TwiddleTables tw, uint32_t* out, cudaStream_t st) {
+  uint64_t h = 1ull << (log_len - 1);
+  if (field == 0)
+    k_fri_fold<KoalaBear><<<blocks_for(h, 256), 256, 0, st>>>(cw, log_len, beta, tw, out);
+  else
+    k_fri_fold<BabyBear><<<blocks_for(h, 256), 256, 0, st>>>(cw, log_len, beta, tw, out);
+  return cudaGetLastError();
+}
+
+// Duplex challenger (challenger.rs:89-115, 202-237), one thread.
+template <class F>
+__device__ void ch_duplex(DevChallenger* ch) {
+  uint32_t s[16];
+  for (int i = 0; i < 16; i++) s[i] = ch->sponge[i];
+  for (uint32_t i = 0; i < ch->in_len; i++) s[i] = ch->in_buf[i];
+  ch->in_len = 0;
+  p2_permute<F>(s);
+  for (int i = 0; i < 16; i++) ch->sponge[i] = s[i];
+  for (int i = 0; i < 8; i++) ch->out_buf[i] = s[i];
+  ch->out_len = 8;
+}
+
+template <class F>
+__device__ void ch_observe(DevChallenger* ch, uint32_t v) {
+  ch->out_len = 0;
+  ch->in_buf[ch->in_len++] = v;
+  if (ch->in_len == 8) ch_duplex<F>(ch);
+}
+
+template <class F>
+__device__ uint32_t ch_sample(DevChallenger* ch) {
+  if (ch->in_len != 0 || ch->out_len == 0) ch_duplex<F>(ch);
+  return ch->out_buf[--ch->out_len];
+}
+
+template <class F>
+__global__ void k_challenger_round(DevChallenger* ch, const uint32_t* root, uint32_t* beta_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = 0; i < 8; i++) ch_observe<F>(ch, root[i]);
+  for (int i = 0; i < 4; i++) beta_out[i] = ch_sample<F>(ch);
+}
+
+template <class F>
+__global__ void k_challenger_observe(DevChallenger* ch, const uint32_t* vals, uint32_t n) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (uint32_t i = 0; i < n; i++) ch_observe<F>(ch, vals[i]);
+}
+
+cudaError_t launch_challenger_round(int field, DevChallenger* ch, const uint32_t* root, uint32_t* beta_out,
+                                    cudaStream_t st) {
+  if (field == 0)
+    k_challenger_round<KoalaBear><<<1, 32, 0, st>>>(ch, root, beta_out);
+  else
+    k_challenger_round<BabyBear><<<1, 32, 0, st>>>(ch, root, beta_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_challenger_observe(int field, DevChallenger* ch, const uint32_t* vals, uint32_t n,
+                                      cudaStream_t st) {
+  if (field == 0)
+    k_challenger_observe<KoalaBear><<<1, 32, 0, st>>>(ch, vals, n);
+  else
+    k_challenger_observe<BabyBear><<<1, 32, 0, st>>>(ch, vals, n);
+  return cudaGetLastError();
+}
+
+}  // namespace pico
+
+namespace pico {
+
+// Final polynomial of the commit phase when folding stops early: the
+// remaining codeword holds 2^log_len evaluations in bit-reversed order; its
+// coefficients over the subgroup are c_i = (1/len) sum_j v[rev(j)] w^(-ij).
+// Coefficients at i >= 2^log_keep must vanish (low-degree check): a nonzero
+// one sets *err.
+template <class F>
+__global__ void k_fri_final_poly(const uint32_t* cw, uint32_t log_len, uint32_t log_keep, TwiddleTables tw,
+                                 uint32_t* coeffs, uint32_t* err) {
+  using B = Fp<F>;
+  const uint32_t len = 1u << log_len;
+  const uint32_t mask = (1u << F::TWO_ADICITY) - 1u;
+  const uint32_t len_inv = B::inv(B::to_monty(len));
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+    uint32_t acc[4] = {0, 0, 0, 0};
+    for (uint32_t j = 0; j < len; j++) {
+      uint32_t e = (uint32_t)(((uint64_t)i * j) & (len - 1)) << (F::TWO_ADICITY - log_len);
+      e = (0u - e) & mask;
+      const uint32_t wv = B::mul(__ldg(tw.hi + (e >> 14)), __ldg(tw.lo + (e & 0x3fffu)));
+      const uint32_t* v = cw + 4 * bitrev32(j, log_len);
+#pragma unroll
+      for (int k = 0; k < 4; k++) acc[k] = B::add(acc[k], B::mul(v[k], wv));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) acc[k] = B::mul(acc[k], len_inv);
+    if (i < (1u << log_keep)) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) coeffs[4 * i + k] = acc[k];
+    } else if (acc[0] | acc[1] | acc[2] | acc[3]) {
+      atomicExch(err, 1u);
+    }
+  }
+}
+
+cudaError_t launch_fri_final_poly(int field, const uint32_t* cw, uint32_t log_len, uint32_t log_keep,
+                                  TwiddleTables tw, uint32_t* coeffs, uint32_t* err, cudaStream_t st) {
+  if (field == 0)
+    k_fri_final_poly<KoalaBear><<<1, 256, 0, st>>>(cw, log_len, log_keep, tw, coeffs, err);
+  else
+    k_fri_final_poly<BabyBear><<<1, 256, 0, st>>>(cw, log_len, log_keep, tw, coeffs, err);
+  return cudaGetLastError();
+}
+
+}  // namespace pico

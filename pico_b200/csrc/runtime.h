@@ -1,0 +1,113 @@
+// Host runtime shared by the C-ABI translation units: context, device memory,
+// commit planning and enqueueing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/pico_gpu.h"
+#include "internal.h"
+
+namespace pico {
+
+void set_error(const char* fmt, ...);
+pico_status cuda_status(cudaError_t e, const char* what);
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// One matrix of a commit after planning.
+struct PlannedMat {
+  uint32_t input_idx;  // position in the caller's array
+  uint32_t log_n;      // trace height (log)
+  uint32_t log_N;      // committed (LDE) height (log)
+  uint32_t w;
+  uint32_t shift;      // Monty
+  const uint32_t* src; // caller's input pointer (host or device)
+};
+
+struct CommitPlan {
+  int field = 0;
+  uint32_t log_b = 0;
+  bool extend = true;            // false: mmcs_commit of already-extended matrices
+  bool input_device = false;
+  bool plain = false;
+  std::vector<PlannedMat> mats;  // in commit order (stable, tallest first)
+  // height groups in commit order: [begin, end) into mats
+  std::vector<std::pair<uint32_t, uint32_t>> groups;
+  uint32_t log_max = 0;
+  uint64_t bytes_resident = 0;   // LDEs + digest layers
+  uint64_t bytes_scratch = 0;    // input copies, NTT scratch, tables
+  uint64_t cells = 0;            // sum of trace cells
+  uint64_t lde_cells = 0;
+  uint64_t permutations = 0;     // tree permutations
+  uint64_t leaf_permutations = 0;
+};
+
+pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t log_b, uint32_t flags, bool extend,
+                        CommitPlan& plan);
+
+struct Server;  // serving.h
+
+bool try_reserve(pico_ctx* ctx, uint64_t bytes);
+void unreserve(pico_ctx* ctx, uint64_t bytes);
+cudaStream_t pick_stream(pico_ctx* ctx);
+TwiddleTables twiddles(pico_ctx* ctx, int field);
+pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, pico_commit* c,
+                           std::vector<void*>& scratch, uint32_t* root_host);
+void free_commit_buffers(pico_commit* c, cudaStream_t st);
+pico_status finish_stats(pico_commit* c);
+
+}  // namespace pico
+
+struct pico_ctx {
+  int device = 0;
+  int sm_count = 0;
+  uint64_t budget = 0;
+  uint64_t reserved = 0;
+  std::mutex mu;               // guards budget accounting
+  std::condition_variable cv;  // signalled whenever reserved memory is returned
+  std::vector<cudaStream_t> streams;
+  std::atomic<uint32_t> next_stream{0};
+  uint32_t* tw[2] = {nullptr, nullptr};  // per-field twiddle tables (lo | hi)
+  pico::Server* server = nullptr;
+  ~pico_ctx();
+};
+
+// Opaque public handles.
+struct pico_commit {
+  pico_ctx* ctx = nullptr;
+  int field = 0;
+  uint32_t log_max = 0;
+  uint32_t n_mats = 0;
+  std::vector<uint32_t*> lde;     // per input index: device LDE (bit-reversed rows)
+  std::vector<uint32_t> log_N;    // per input index
+  std::vector<uint32_t> width;    // per input index
+  std::vector<bool> owns;         // whether lde[i] is owned by the commit
+  uint32_t* layers = nullptr;     // all digest layers, leaves first
+  uint64_t bytes_resident = 0;
+  uint32_t root[8] = {0};
+  // events: start, inputs copied, LDE done, leaves done, tree done
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  pico_commit_stats stats{};
+  ~pico_commit();
+};
+
+struct pico_fri {
+  pico_ctx* ctx = nullptr;
+  int field = 0;
+  uint32_t log_n = 0, rounds = 0;
+  std::vector<uint32_t*> codewords;  // round r: 2^(log_n - r) x 4
+  std::vector<uint32_t*> trees;      // round r: digest layers over 2^(log_n - r - 1) leaves
+  uint64_t bytes_resident = 0;
+};

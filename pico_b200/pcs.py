@@ -1,0 +1,378 @@
+"""Host-side mirror of the prover's commitment interface, over the C ABI.
+
+Names and argument meanings follow the Plonky3 types the reference binds in
+vm/src/configs/stark_config/kb_poseidon2.rs:15-27 (and bb_poseidon2.rs):
+TwoAdicFriPcs (commit, get_evaluations_on_domain, the FRI commit phase),
+MerkleTreeMmcs (commit, open_batch), Radix2DitParallel (coset_lde_batch) and
+the Poseidon2 permutation.  Errors surface as PicoError with the library's
+status code and message, the way the Rust shim would panic on misuse.
+
+Matrices are numpy uint32 arrays (host, Monty form) or CUDA tensors whose
+int32/uint32 storage holds the same bit patterns (device).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from . import fields as F
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+def _ptr(a) -> int:
+    if _is_device(a):
+        if not a.is_contiguous():
+            raise ValueError("device matrices must be contiguous")
+        return a.data_ptr()
+    if not (isinstance(a, np.ndarray) and a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]):
+        raise ValueError("host matrices must be C-contiguous numpy uint32 arrays")
+    return a.ctypes.data
+
+
+def _log2_exact(n: int) -> int:
+    if n <= 0 or n & (n - 1):
+        raise ValueError(f"height {n} is not a power of two")
+    return n.bit_length() - 1
+
+
+class GpuContext:
+    """One device context (pico_gpu_init).  Thread-safe; close() when done."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, n_streams: int = 0):
+        self.lib = abi.load()
+        cfg = abi.Config()
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        cfg.n_streams = n_streams
+        h = C.c_void_p()
+        abi.check(self.lib.pico_gpu_init(device, C.byref(cfg), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            abi.check(self.lib.pico_gpu_shutdown(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def memory(self):
+        r, b = C.c_uint64(), C.c_uint64()
+        abi.check(self.lib.pico_gpu_memory(self.handle, C.byref(r), C.byref(b)))
+        return r.value, b.value
+
+
+@dataclass
+class TwoAdicDomain:
+    """TwoAdicMultiplicativeCoset: shift * <w_{2^log_n}> (shift canonical)."""
+
+    log_n: int
+    shift: int = 1
+
+
+class ProverData:
+    """Resident prover data of one commit (pico_commit): LDEs + digest layers."""
+
+    def __init__(self, ctx: GpuContext, handle: C.c_void_p, root: np.ndarray, n_mats: int, field: int):
+        self.ctx, self.handle, self.root, self.n_mats, self.field = ctx, handle, root, n_mats, field
+
+    def release(self):
+        if self.handle:
+            abi.check(self.ctx.lib.pico_gpu_release(self.ctx.handle, self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            if self.handle and self.ctx.handle:
+                self.release()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        st = abi.CommitStats()
+        abi.check(self.ctx.lib.pico_gpu_commit_stats(self.handle, C.byref(st)))
+        return st.as_dict()
+
+    def lde_shape(self, i: int):
+        lh, w = C.c_uint32(), C.c_uint32()
+        abi.check(self.ctx.lib.pico_gpu_lde_shape(self.handle, i, C.byref(lh), C.byref(w)))
+        return 1 << lh.value, w.value
+
+    @property
+    def log_max_height(self) -> int:
+        return max(self.lde_shape(i)[0] for i in range(self.n_mats)).bit_length() - 1
+
+    def lde_rows(self, i: int, begin: int = 0, end: int | None = None, out=None):
+        """Committed (bit-reversed) rows [begin, end) of LDE i; host numpy unless `out` is a CUDA tensor."""
+        h, w = self.lde_shape(i)
+        end = h if end is None else end
+        flags = 0
+        if out is None:
+            out = np.empty((end - begin, w), dtype=np.uint32)
+        if _is_device(out):
+            flags |= abi.PICO_OUTPUT_DEVICE
+        abi.check(self.ctx.lib.pico_gpu_lde_rows(self.ctx.handle, self.handle, i, begin, end, _ptr(out), flags))
+        return out
+
+    def lde(self, i: int):
+        return self.lde_rows(i)
+
+    def digest_layer(self, level: int) -> np.ndarray:
+        n = 1 << (self.log_max_height - level)
+        out = np.empty((n, 8), dtype=np.uint32)
+        abi.check(self.ctx.lib.pico_gpu_digest_layer(self.ctx.handle, self.handle, level, out.ctypes.data, 0))
+        return out
+
+
+class MerkleTreeMmcs:
+    """MerkleTreeMmcs<_, _, PaddingFreeSponge<Perm,16,8,8>, TruncatedPermutation<Perm,2,8,16>, 8>."""
+
+    def __init__(self, ctx: GpuContext, field):
+        self.ctx, self.field = ctx, F.field_id(field)
+
+    def commit(self, matrices, plain: bool = False):
+        mats = (abi.Matrix * len(matrices))()
+        flags = abi.PICO_COMMIT_PLAIN if plain else 0
+        dev = [_is_device(m) for m in matrices]
+        if any(dev) and not all(dev):
+            raise ValueError("matrices must be all host or all device")
+        if all(dev):
+            flags |= abi.PICO_INPUT_DEVICE
+        for k, m in enumerate(matrices):
+            mats[k].values = _ptr(m)
+            mats[k].log_height = _log2_exact(m.shape[0])
+            mats[k].width = m.shape[1]
+        root = np.zeros(8, dtype=np.uint32)
+        h = C.c_void_p()
+        abi.check(self.ctx.lib.pico_gpu_mmcs_commit(
+            self.ctx.handle, self.field, mats, len(matrices), flags, C.byref(h),
+            root.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return root, ProverData(self.ctx, h, root, len(matrices), self.field)
+
+    def open_batch(self, index: int, prover_data: ProverData):
+        """(opened rows per matrix, sibling path) at `index` of the tallest matrix."""
+        widths = [prover_data.lde_shape(i)[1] for i in range(prover_data.n_mats)]
+        rows = np.zeros(sum(widths), dtype=np.uint32)
+        path = np.zeros((prover_data.log_max_height, 8), dtype=np.uint32)
+        abi.check(self.ctx.lib.pico_gpu_open_batch(self.ctx.handle, prover_data.handle, index,
+                                                   rows.ctypes.data, path.ctypes.data))
+        out, off = [], 0
+        for w in widths:
+            out.append(rows[off:off + w].copy())
+            off += w
+        return out, path
+
+
+class Radix2DitParallel:
+    """SC_Dft: coset LDE of a batch of columns."""
+
+    def __init__(self, ctx: GpuContext, field):
+        self.ctx, self.field = ctx, F.field_id(field)
+
+    def coset_lde_batch_bitrev(self, mat, added_bits: int, shift_monty: int, out=None):
+        """LDE rows in the committed (bit-reversed) order."""
+        n, w = mat.shape
+        flags = abi.PICO_INPUT_DEVICE if _is_device(mat) else 0
+        if out is None:
+            out = np.empty((n << added_bits, w), dtype=np.uint32)
+        if _is_device(out):
+            flags |= abi.PICO_OUTPUT_DEVICE
+        abi.check(self.ctx.lib.pico_gpu_coset_lde_batch(self.ctx.handle, self.field, _ptr(mat), _log2_exact(n), w,
+                                                        added_bits, shift_monty, _ptr(out), flags))
+        return out
+
+    def coset_lde_batch(self, mat, added_bits: int, shift_monty: int) -> np.ndarray:
+        """Natural row order, as the Dft trait returns it (host result)."""
+        br = self.coset_lde_batch_bitrev(mat, added_bits, shift_monty)
+        logn = _log2_exact(br.shape[0])
+        idx = np.arange(br.shape[0])
+        rev = np.zeros_like(idx)
+        for b in range(logn):
+            rev |= ((idx >> b) & 1) << (logn - 1 - b)
+        return br[rev]
+
+
+class Poseidon2:
+    def __init__(self, ctx: GpuContext, field):
+        self.ctx, self.field = ctx, F.field_id(field)
+
+    def permute(self, states):
+        """In place on (n, 16) states (host numpy or CUDA tensor)."""
+        flags = abi.PICO_INPUT_DEVICE if _is_device(states) else 0
+        abi.check(self.ctx.lib.pico_gpu_poseidon2_permute(self.ctx.handle, self.field, _ptr(states),
+                                                          states.shape[0], flags))
+        return states
+
+
+@dataclass
+class FriCommitResult:
+    roots: np.ndarray
+    betas: np.ndarray
+    final_poly: np.ndarray
+    rounds: int
+    data: "FriData | None"
+
+
+class FriData:
+    def __init__(self, ctx, handle, log_n):
+        self.ctx, self.handle, self.log_n = ctx, handle, log_n
+
+    def layer(self, r: int) -> np.ndarray:
+        out = np.empty(((1 << (self.log_n - r)), 4), dtype=np.uint32)
+        abi.check(self.ctx.lib.pico_gpu_fri_layer(self.ctx.handle, self.handle, r, out.ctypes.data, 0))
+        return out
+
+    def release(self):
+        if self.handle:
+            abi.check(self.ctx.lib.pico_gpu_fri_release(self.ctx.handle, self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            if self.handle and self.ctx.handle:
+                self.release()
+        except Exception:
+            pass
+
+
+def last_commit_stats() -> dict:
+    """Device timings of the calling thread's last synchronous commit."""
+    st = abi.CommitStats()
+    abi.check(abi.load().pico_gpu_last_commit_stats(C.byref(st)))
+    return st.as_dict()
+
+
+def new_challenger() -> abi.Challenger:
+    """DuplexChallenger::new: zero sponge, empty buffers."""
+    return abi.Challenger()
+
+
+class TwoAdicFriPcs:
+    """SC_Pcs = TwoAdicFriPcs<Val, Dft, ValMmcs, ChallengeMmcs>."""
+
+    def __init__(self, ctx: GpuContext, field, log_blowup: int):
+        self.ctx, self.field, self.log_blowup = ctx, F.field_id(field), log_blowup
+
+    def natural_domain_for_degree(self, n: int) -> TwoAdicDomain:
+        return TwoAdicDomain(_log2_exact(n), 1)
+
+    def commit(self, domains_and_traces, plain: bool = False, keep: bool = True):
+        """[(domain, trace)] -> (root, ProverData).  LDE shift per matrix is
+        GENERATOR / domain.shift, as TwoAdicFriPcs::commit computes it."""
+        n = len(domains_and_traces)
+        mats = (abi.Matrix * n)()
+        flags = abi.PICO_COMMIT_PLAIN if plain else 0
+        traces = [t for _, t in domains_and_traces]
+        dev = [_is_device(t) for t in traces]
+        if any(dev) and not all(dev):
+            raise ValueError("traces must be all host or all device")
+        if all(dev):
+            flags |= abi.PICO_INPUT_DEVICE
+        for k, (dom, t) in enumerate(domains_and_traces):
+            if t.shape[0] != 1 << dom.log_n:
+                raise ValueError(f"trace {k}: height {t.shape[0]} != domain size {1 << dom.log_n}")
+            mats[k].values = _ptr(t)
+            mats[k].log_height = dom.log_n
+            mats[k].width = t.shape[1]
+            mats[k].shift = F.lde_shift(self.field, dom.shift)
+        root = np.zeros(8, dtype=np.uint32)
+        h = C.c_void_p()
+        abi.check(self.ctx.lib.pico_gpu_commit(
+            self.ctx.handle, self.field, mats, n, self.log_blowup, flags,
+            C.byref(h) if keep else None, root.ctypes.data_as(C.POINTER(C.c_uint32))))
+        pd = ProverData(self.ctx, h, root, n, self.field) if keep else None
+        return root, pd
+
+    def get_evaluations_on_domain(self, prover_data: ProverData, idx: int):
+        """The committed LDE of matrix idx (bit-reversed rows, as stored)."""
+        return prover_data.lde(idx)
+
+    def fri_commit_phase(self, codeword, log_final_len: int = 0, betas=None, challenger=None,
+                         keep: bool = False) -> FriCommitResult:
+        """FRI commit phase over an EF4 codeword ((2^k, 4) Monty words, bit-reversed order)."""
+        log_n = _log2_exact(codeword.shape[0])
+        rounds = log_n - self.log_blowup - log_final_len
+        if rounds < 0:
+            raise ValueError("codeword shorter than the final length")
+        flags = abi.PICO_INPUT_DEVICE if _is_device(codeword) else 0
+        roots = np.zeros((max(rounds, 1), 8), dtype=np.uint32)
+        out_betas = np.zeros((max(rounds, 1), 4), dtype=np.uint32)
+        final = np.zeros((1 << log_final_len, 4), dtype=np.uint32)
+        if betas is not None:
+            betas = np.ascontiguousarray(betas, dtype=np.uint32)
+        ch = challenger if challenger is not None else (new_challenger() if betas is None else None)
+        nr = C.c_uint32()
+        h = C.c_void_p()
+        abi.check(self.ctx.lib.pico_gpu_fri_commit_phase(
+            self.ctx.handle, self.field, _ptr(codeword), log_n, self.log_blowup, log_final_len,
+            betas.ctypes.data if betas is not None else None,
+            C.byref(ch) if ch is not None else None, flags, roots.ctypes.data, out_betas.ctypes.data,
+            final.ctypes.data, C.byref(nr), C.byref(h) if keep else None))
+        data = FriData(self.ctx, h, log_n) if keep else None
+        return FriCommitResult(roots[:rounds], out_betas[:rounds], final, nr.value, data)
+
+
+class CommitRequest:
+    def __init__(self, server: "CommitServer", handle: C.c_void_p, n_mats: int, field: int):
+        self.server, self.handle, self.n_mats, self.field = server, handle, n_mats, field
+
+    def poll(self) -> bool:
+        s = self.server.ctx.lib.pico_gpu_poll(self.server.ctx.handle, self.handle)
+        if s == 6:  # PICO_ERR_NOT_READY
+            return False
+        abi.check(s)
+        return True
+
+    def wait(self, timeout_ms: int = -1, keep: bool = True):
+        root = np.zeros(8, dtype=np.uint32)
+        h = C.c_void_p()
+        abi.check(self.server.ctx.lib.pico_gpu_wait(
+            self.server.ctx.handle, self.handle, timeout_ms, C.byref(h) if keep else None,
+            root.ctypes.data_as(C.POINTER(C.c_uint32))))
+        pd = ProverData(self.server.ctx, h, root, self.n_mats, self.field) if keep else None
+        return root, pd
+
+    def times(self):
+        q, r = C.c_double(), C.c_double()
+        abi.check(self.server.ctx.lib.pico_gpu_request_times(self.handle, C.byref(q), C.byref(r)))
+        return q.value, r.value
+
+    def cancel(self):
+        abi.check(self.server.ctx.lib.pico_gpu_cancel(self.server.ctx.handle, self.handle))
+
+    def free(self):
+        if self.handle:
+            abi.check(self.server.ctx.lib.pico_gpu_request_free(self.server.ctx.handle, self.handle))
+            self.handle = None
+
+
+class CommitServer:
+    """Serving front end: asynchronous commits admitted by free HBM."""
+
+    def __init__(self, ctx: GpuContext):
+        self.ctx = ctx
+
+    def submit(self, field, traces, log_blowup: int, shifts=None) -> CommitRequest:
+        f = F.field_id(field)
+        n = len(traces)
+        mats = (abi.Matrix * n)()
+        dev = [_is_device(t) for t in traces]
+        if any(dev) and not all(dev):
+            raise ValueError("traces must be all host or all device")
+        flags = abi.PICO_INPUT_DEVICE if all(dev) else 0
+        for k, t in enumerate(traces):
+            mats[k].values = _ptr(t)
+            mats[k].log_height = _log2_exact(t.shape[0])
+            mats[k].width = t.shape[1]
+            mats[k].shift = shifts[k] if shifts is not None else F.lde_shift(f)
+        h = C.c_void_p()
+        abi.check(self.ctx.lib.pico_gpu_submit_commit(self.ctx.handle, f, mats, n, log_blowup, flags, C.byref(h)))
+        return CommitRequest(self, h, n, f)

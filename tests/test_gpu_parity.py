@@ -1,0 +1,277 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Integer field arithmetic: every comparison is bit-exact.  Small and medium
+shapes compare whole outputs with the oracle; the full-size batched shape is
+checked through size-independent properties (LDE column slices against the
+oracle, Merkle openings verified with the oracle's hash and compression,
+batched == per-matrix form).
+"""
+import numpy as np
+import pytest
+
+from pico_b200 import (CommitServer, MerkleTreeMmcs, PicoError, Poseidon2, Radix2DitParallel, TwoAdicDomain,
+                       TwoAdicFriPcs)
+from pico_b200 import fields as F
+
+pytestmark = pytest.mark.gpu
+FIELDS = [0, 1]
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def to_dev(a):
+    torch = _torch()
+    return torch.from_numpy(a.view(np.int32)).cuda()
+
+
+# ---------------------------------------------------------------- Poseidon2
+@pytest.mark.parametrize("f", FIELDS)
+def test_permute_kat_and_random(gpu, orc, golden, f):
+    name = F.NAMES[f]
+    zero = np.zeros((1, 16), dtype=np.uint32)
+    Poseidon2(gpu, f).permute(zero)
+    assert F.from_monty(f, zero[0]).tolist() == golden["kat"][name]["output"]
+    st = F.to_monty(f, F.uniform(f, 16 * 1000, 5)).reshape(1000, 16)
+    want = orc.permute(f, st)
+    got = st.copy()
+    Poseidon2(gpu, f).permute(got)
+    assert (got == want).all()
+    d = to_dev(st.copy())
+    Poseidon2(gpu, f).permute(d)
+    assert (d.cpu().numpy().view(np.uint32) == want).all()
+
+
+# ---------------------------------------------------------------- coset LDE
+LDE_SHAPES = [(0, 3, 1), (1, 1, 1), (3, 2, 2), (4, 3, 2), (7, 9, 1), (10, 8, 1), (11, 13, 1), (11, 1, 3),
+              (12, 5, 1), (12, 8, 2), (13, 8, 1), (14, 33, 1), (15, 2, 2), (16, 3, 1), (17, 12, 1)]
+
+
+@pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("logn,w,b", LDE_SHAPES)
+def test_coset_lde(gpu, orc, f, logn, w, b):
+    m = F.random_matrix(f, logn, w, 300 + logn * 7 + w)
+    shift = F.lde_shift(f)
+    want = orc.coset_lde(f, m, b, shift)
+    got = Radix2DitParallel(gpu, f).coset_lde_batch_bitrev(m, b, shift)
+    assert got.shape == want.shape
+    assert (got == want).all()
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_coset_lde_arbitrary_shift_and_natural_order(gpu, orc, f):
+    m = F.random_matrix(f, 9, 6, 17)
+    shift = F.to_monty(f, [123456789])[0]
+    want = orc.coset_lde(f, m, 2, int(shift), bitrev=False)
+    got = Radix2DitParallel(gpu, f).coset_lde_batch(m, 2, int(shift))
+    assert (got == want).all()
+
+
+def test_coset_lde_device_buffers(gpu, orc):
+    torch = _torch()
+    f = 0
+    m = F.random_matrix(f, 13, 16, 8)
+    out = torch.empty((1 << 14, 16), dtype=torch.int32, device="cuda")
+    Radix2DitParallel(gpu, f).coset_lde_batch_bitrev(to_dev(m), 1, F.lde_shift(f), out=out)
+    assert (out.cpu().numpy().view(np.uint32) == orc.coset_lde(f, m, 1, F.lde_shift(f))).all()
+
+
+# ---------------------------------------------------------------- commits
+def commit_both(gpu, orc, f, shapes, b, seed0, plain=False, device=False):
+    mats = [F.random_matrix(f, lh, w, seed0 + i) for i, (lh, w) in enumerate(shapes)]
+    want_root, want_ldes, want_layers = orc.pcs_commit(f, mats, [F.lde_shift(f)] * len(mats), b, want_ldes=True,
+                                                       want_layers=True)
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    ins = [to_dev(m) for m in mats] if device else mats
+    root, pd = pcs.commit([(pcs.natural_domain_for_degree(m.shape[0]), m) for m in ins], plain=plain)
+    return mats, root, pd, want_root, want_ldes, want_layers
+
+
+@pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("plain", [False, True])
+def test_commit_golden_shapes(gpu, orc, golden, f, plain):
+    pc = golden["vectors"][F.NAMES[f]]["pcs_commit"]
+    mats = [F.random_matrix(f, lh, w, s) for lh, w, s in pc["shapes"]]
+    pcs = TwoAdicFriPcs(gpu, f, pc["log_blowup"])
+    root, pd = pcs.commit([(TwoAdicDomain(m.shape[0].bit_length() - 1), m) for m in mats], plain=plain)
+    assert root.tolist() == pc["root"]
+    pd.release()
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_commit_single_matrix_config1(gpu, orc, f):
+    """One 2^16 x 64 trace, log_blowup 1: the plain single-matrix commit."""
+    mats, root, pd, want_root, want_ldes, want_layers = commit_both(gpu, orc, f, [(16, 64)], 1, 1)
+    assert root.tolist() == want_root.tolist()
+    assert (pd.lde(0) == want_ldes[0]).all()
+    assert (pd.digest_layer(0) == want_layers[: 1 << 17]).all()
+
+
+@pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("b", [1, 2])
+def test_commit_uneven_batch(gpu, orc, f, b):
+    rng = np.random.default_rng(7 + f + b)
+    shapes = [(int(rng.integers(4, 15)), int(rng.integers(1, 120))) for _ in range(24)]
+    shapes += [(14, 8), (14, 3), (9, 400), (0, 5)]
+    for plain in (False, True):
+        mats, root, pd, want_root, want_ldes, want_layers = commit_both(gpu, orc, f, shapes, b, 500, plain=plain)
+        assert root.tolist() == want_root.tolist()
+        for i in range(len(mats)):
+            assert (pd.lde(i) == want_ldes[i]).all()
+        log_max = max(s[0] for s in shapes) + b
+        off = 0
+        for lvl in range(log_max + 1):
+            n = 1 << (log_max - lvl)
+            assert (pd.digest_layer(lvl) == want_layers[off:off + n]).all()
+            off += n
+        pd.release()
+
+
+def test_commit_device_inputs_and_rows(gpu, orc):
+    f = 0
+    shapes = [(12, 20), (10, 7), (12, 9)]
+    mats, root, pd, want_root, want_ldes, _ = commit_both(gpu, orc, f, shapes, 1, 900, device=True)
+    assert root.tolist() == want_root.tolist()
+    assert (pd.lde_rows(1, 100, 300) == want_ldes[1][100:300]).all()
+    torch = _torch()
+    out = torch.empty((50, 20), dtype=torch.int32, device="cuda")
+    pd.lde_rows(0, 7, 57, out=out)
+    assert (out.cpu().numpy().view(np.uint32) == want_ldes[0][7:57]).all()
+
+
+def verify_batch(orc, f, root, heights, index, opened, path):
+    """MMCS opening check restated from the verifier (fri.rs:389-436)."""
+    order = sorted(range(len(heights)), key=lambda i: -heights[i])
+    log_max = heights[order[0]].bit_length() - 1
+    cur_h = heights[order[0]]
+    k = 0
+    elems = []
+    while k < len(order) and heights[order[k]] == cur_h:
+        elems.append(opened[order[k]])
+        k += 1
+    node = orc.hash_elems(f, np.concatenate(elems) if elems else np.zeros(0, np.uint32))
+    for lvl in range(log_max):
+        bit = (index >> lvl) & 1
+        sib = path[lvl]
+        node = orc.compress(f, sib, node) if bit else orc.compress(f, node, sib)
+        cur_h //= 2
+        elems = []
+        while k < len(order) and heights[order[k]] == cur_h:
+            elems.append(opened[order[k]])
+            k += 1
+        if elems:
+            node = orc.compress(f, node, orc.hash_elems(f, np.concatenate(elems)))
+    return node.tolist() == list(root)
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_open_batch_verifies(gpu, orc, f):
+    shapes = [(10, 5), (8, 3), (10, 2), (6, 11)]
+    mats, root, pd, want_root, want_ldes, _ = commit_both(gpu, orc, f, shapes, 1, 40)
+    assert root.tolist() == want_root.tolist()
+    mmcs = MerkleTreeMmcs(gpu, f)
+    heights = [pd.lde_shape(i)[0] for i in range(len(mats))]
+    for index in (0, 1, 777, (1 << 11) - 1):
+        rows, path = mmcs.open_batch(index, pd)
+        for i, r in enumerate(rows):
+            assert (r == want_ldes[i][index >> (11 - heights[i].bit_length() + 1)]).all()
+        assert verify_batch(orc, f, root, heights, index, rows, path)
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_mmcs_commit_prebuilt_matrices(gpu, orc, f):
+    mats = [F.random_matrix(f, 9, 3, 1), F.random_matrix(f, 7, 10, 2), F.random_matrix(f, 9, 16, 3)]
+    want = orc.mmcs_commit(f, mats)
+    root, pd = MerkleTreeMmcs(gpu, f).commit(mats)
+    assert root.tolist() == want.tolist()
+    root2, _ = MerkleTreeMmcs(gpu, f).commit([to_dev(m) for m in mats])
+    assert root2.tolist() == want.tolist()
+
+
+def test_invalid_shapes_are_reported(gpu):
+    import ctypes as C
+
+    from pico_b200 import abi
+
+    pcs = TwoAdicFriPcs(gpu, 0, 1)
+    with pytest.raises(ValueError):  # trace height differs from its domain
+        pcs.commit([(TwoAdicDomain(4), np.zeros((10, 2), np.uint32))])
+    m = np.zeros((16, 2), dtype=np.uint32)
+    mats = (abi.Matrix * 1)()
+    mats[0].values = m.ctypes.data
+    mats[0].log_height = 23
+    mats[0].width = 2
+    root = (C.c_uint32 * 8)()
+    # 2^23 rows with blowup 4 exceeds KoalaBear's two-adicity 24
+    with pytest.raises(PicoError):
+        abi.check(gpu.lib.pico_gpu_commit(gpu.handle, 0, mats, 1, 2, 0, None, root))
+
+
+# ---------------------------------------------------------------- FRI
+def ef4_codeword(f, log_trace, b, seed):
+    base = F.random_matrix(f, log_trace, 4, seed)
+    import oracle.cpu as o
+
+    return o.coset_lde(f, base, b, F.lde_shift(f))
+
+
+@pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("log_trace,b", [(5, 1), (10, 1), (9, 2), (14, 1)])
+def test_fri_commit_phase_challenger(gpu, orc, f, log_trace, b):
+    cw = ef4_codeword(f, log_trace, b, 60 + log_trace)
+    roots, betas, final, ch = orc.fri_commit_phase(f, cw, b)
+    res = TwoAdicFriPcs(gpu, f, b).fri_commit_phase(cw)
+    assert res.rounds == log_trace
+    assert (res.roots == roots).all()
+    assert (res.betas == betas).all()
+    assert (res.final_poly[0] == final[0]).all()
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_fri_commit_phase_explicit_betas_and_early_stop(gpu, orc, f):
+    b = 1
+    cw = ef4_codeword(f, 11, b, 70)
+    betas = F.to_monty(f, F.uniform(f, 4 * 11, 71)).reshape(11, 4)
+    roots, _, final, _ = orc.fri_commit_phase(f, cw, b, 0, betas=betas)
+    res = TwoAdicFriPcs(gpu, f, b).fri_commit_phase(cw, betas=betas)
+    assert (res.roots == roots).all() and (res.final_poly[0] == final[0]).all()
+    roots4, betas4, final4, _ = orc.fri_commit_phase(f, cw, b, 4)
+    res4 = TwoAdicFriPcs(gpu, f, b).fri_commit_phase(cw, log_final_len=4, keep=True)
+    assert (res4.roots == roots4).all() and (res4.betas == betas4).all()
+    assert (res4.final_poly == final4).all()
+    assert (res4.data.layer(0) == cw).all()
+    res4.data.release()
+
+
+def test_fri_rejects_high_degree_codeword(gpu):
+    cw = F.to_monty(0, F.uniform(0, 4 * 64, 3)).reshape(64, 4)  # random: not low degree
+    with pytest.raises(PicoError):
+        TwoAdicFriPcs(gpu, 0, 1).fri_commit_phase(cw)
+
+
+# ---------------------------------------------------------------- serving
+def test_serving_results_match_alone(gpu, orc):
+    """Each request's root is the same when run alone and in a concurrent mix."""
+    server = CommitServer(gpu)
+    rng = np.random.default_rng(3)
+    reqs = []
+    for k in range(12):
+        f = int(rng.random() < 0.3)
+        b = int(rng.integers(1, 3))
+        shapes = [(int(rng.integers(3, 13)), int(rng.integers(1, 64))) for _ in range(int(rng.integers(1, 6)))]
+        mats = [F.random_matrix(f, lh, w, 1000 * k + i) for i, (lh, w) in enumerate(shapes)]
+        reqs.append((f, b, mats, server.submit(f, mats, b)))
+    for f, b, mats, r in reqs:
+        root, pd = r.wait(timeout_ms=60000)
+        alone, _ = TwoAdicFriPcs(gpu, f, b).commit([(TwoAdicDomain(m.shape[0].bit_length() - 1), m) for m in mats],
+                                                   keep=False)
+        want, _, _ = orc.pcs_commit(f, mats, [F.lde_shift(f)] * len(mats), b)
+        assert root.tolist() == alone.tolist() == want.tolist()
+        q, run = r.times()
+        assert q >= 0 and run > 0
+        pd.release()
+        r.free()
+    assert gpu.memory()[0] == 0
