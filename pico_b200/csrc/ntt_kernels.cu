@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256) k_lde_b(const __grid_constant__ LdeBatch 
   using B = Fp<F>;
   extern __shared__ uint32_t smem[];
   uint32_t local;
-  const LdeMat& M = find_tile(batch, kPassA, blockIdx.x, local);
+  const LdeMat& M = find_tile(batch, kPassB, blockIdx.x, local);
   const uint32_t log_L = M.log_n2, L = 1u << log_L, log_n1 = M.log_n1;
   const uint32_t log_ws = ilog2(M.ws), ws = M.ws;
   const uint32_t log_J = ilog2(M.J);
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(256) k_lde_c(const __grid_constant__ LdeBatch 
                                                const __grid_constant__ TwiddleTables tw) {
   extern __shared__ uint32_t smem[];
   uint32_t local;
-  const LdeMat& M = find_tile(batch, kPassA, blockIdx.x, local);
+  const LdeMat& M = find_tile(batch, kPassC, blockIdx.x, local);
   const uint32_t log_L = M.log_n1, L = 1u << log_L, log_n2 = M.log_n2;
   const uint32_t log_ws = ilog2(M.ws), ws = M.ws;
   const uint32_t log_LW = log_ws + ilog2(M.J);
