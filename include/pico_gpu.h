@@ -156,6 +156,22 @@ pico_status pico_gpu_open_batch(pico_ctx *ctx, const pico_commit *c, uint64_t in
 pico_status pico_gpu_coset_lde_batch(pico_ctx *ctx, pico_field field, const uint32_t *in, uint32_t log_n,
                                      uint32_t width, uint32_t log_blowup, uint32_t shift, uint32_t *out,
                                      uint32_t flags);
+/* Allocation-free variant of pico_gpu_coset_lde_batch.  No counterpart in the
+ * reference: it exists for callers that cannot let this library allocate
+ * device memory (a prover that has reserved all of HBM for its own arena, or
+ * a latency-bound loop that cannot afford cudaMalloc/cudaFree's device-wide
+ * synchronisation).  `in` and `out` are device buffers owned by the caller;
+ * scratch comes from a 32 MiB array declared in device memory by the library
+ * (held by every GPU that loads it until exit), so LDEs needing more than
+ * 2^b*8192 + n*w*(1 + 2^b) > 8 Mi words of scratch are rejected with
+ * PICO_ERR_INVALID_ARG.  No context is needed; work is enqueued on `stream`
+ * (a cudaStream_t, 0 = legacy default) and is complete when the stream
+ * reaches that point.  All calls share the scratch array: calls that overlap
+ * on the GPU race and must be serialised.  The first call on a device does a
+ * one-time set-up (symbol lookup, twiddle fill, synchronise) and should come
+ * before any stream capture. */
+pico_status pico_gpu_coset_lde_batch_noalloc(pico_field field, const uint32_t *in, uint32_t log_n, uint32_t width,
+                                             uint32_t log_blowup, uint32_t shift, uint32_t *out, void *stream);
 /* MerkleTreeMmcs::commit (SC_ValMmcs, kb_poseidon2.rs:19-20) over matrices
  * that are already extended: mats[i].log_height is the matrix's own height,
  * shift is ignored. */
