@@ -59,6 +59,9 @@ def uneven_kb_shapes(seed: int = 2, n: int = 32, target_log: int = 30, lo: int =
 WORKLOADS = {
     "uneven-kb-2^30": dict(field=0, log_blowup=1, shapes=lambda: uneven_kb_shapes(), seed=2),
     "single-kb-2^16x64": dict(field=0, log_blowup=1, shapes=lambda: [(16, 64)], seed=1),
+    # same shape distribution scaled to 2^25 cells (heights 2^6..2^18): for profiler captures
+    "uneven-kb-2^25": dict(field=0, log_blowup=1, shapes=lambda: uneven_kb_shapes(target_log=25, lo=6, hi=18),
+                           seed=2),
 }
 
 

@@ -22,7 +22,7 @@ INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-              "-Xptxas", "-warn-spills"] + ARCH
+              "-Xptxas", "-warn-spills"] + ARCH + os.environ.get("PICO_NVCC_EXTRA", "").split()
 
 
 def _nvcc() -> str:

@@ -72,9 +72,7 @@ struct LdeMat {
   uint32_t* t2;        // N x w scratch (three-pass form only)
   uint32_t* pw;        // 2^b tables of 8192 words: g_cb^i / n, two-level
   uint32_t log_n, log_b, w;
-  uint32_t ws, J;          // column-tile width and adjacent sub-transforms per tile
   uint32_t log_n1, log_n2; // three-pass split n = n1 * n2 (0 for the one-pass form)
-  uint32_t n_ct;           // number of column tiles
   uint32_t shift;          // coset shift, Monty form
 };
 constexpr int kLdeSmallMaxLog = 11;  // one-pass form handles n <= 2^11
@@ -91,7 +89,7 @@ constexpr uint32_t kPwWords = 8192;  // words per (matrix, coset) power table
 cudaError_t launch_lde(int field, const LdeMat* mats, uint32_t n, TwiddleTables tw, cudaStream_t st,
                        uint64_t* launches = nullptr);
 
-// Choose tiling for one matrix (fills ws, J, log_n1, log_n2, n_ct).
+// Choose the one-pass or three-pass form for one matrix (fills log_n1, log_n2).
 void plan_lde_tiling(LdeMat& m);
 
 }  // namespace pico

@@ -19,7 +19,7 @@
 
 namespace pico {
 
-struct P2Constants {
+struct __align__(16) P2Constants {
   uint32_t ext[8][16];  // full-round constants, Monty form: rounds 0..3 then the 4 final rounds
   uint32_t inte[24];    // partial-round constants (lane 0), Monty form
   uint32_t diag[16];    // internal diagonal D_i, Monty form
@@ -59,26 +59,64 @@ __device__ __forceinline__ void p2_external(uint32_t s[16]) {
   for (int i = 0; i < 16; i++) s[i] = B::add(s[i], sums[i & 3]);
 }
 
+// x^3 (KoalaBear) or x^7 (BabyBear) of a canonical x, canonical result.
+// Montgomery products of canonical factors land below 1.5p, so a raw product
+// can feed one more multiply before the single final reduction.
 template <class F>
 __device__ __forceinline__ uint32_t p2_sbox(uint32_t x) {
   using B = Fp<F>;
   if constexpr (F::SBOX == 3) {
-    return B::mul(B::sqr(x), x);
+    const uint32_t x2 = B::redc((uint64_t)x * x);  // < 1.5p
+    return B::canon(B::redc((uint64_t)x2 * x));    // x2 * x < 1.5p^2 -> < 1.75p
   } else {
-    uint32_t x2 = B::sqr(x);
-    uint32_t x3 = B::mul(x2, x);
-    uint32_t x4 = B::sqr(x2);
-    return B::mul(x4, x3);
+    const uint32_t x2 = B::canon(B::redc((uint64_t)x * x));
+    const uint32_t x3 = B::canon(B::redc((uint64_t)x2 * x));
+    const uint32_t x4 = B::redc((uint64_t)x2 * x2);  // < 1.5p
+    return B::canon(B::redc((uint64_t)x4 * x3));     // < 1.75p
   }
 }
 
+// Reduce a 64-bit sum of at most 16 canonical values (< 2^35) to [0, p).
+// With 2^31 = c (mod p): v = hi * 2^31 + lo == lo + hi * c.
 template <class F>
-__device__ __forceinline__ void p2_internal(uint32_t s[16]) {
+__device__ __forceinline__ uint32_t p2_reduce_sum(uint64_t v) {
   using B = Fp<F>;
-  const P2Constants& C = c_p2[F::ID];
-  uint32_t sum = B::add(s[0], s[1]);
+  constexpr uint32_t C = (uint32_t)((1ull << 31) % F::P);  // KB 2^24 - 1, BB 2^27 - 1
+  const uint32_t hi = (uint32_t)(v >> 31), lo = (uint32_t)v & 0x7fffffffu;
+  const uint32_t r = lo + hi * C;  // KB: < 2^31 + 2^28 < 2p; BB: < 2^31 + 15 (2^27 - 1) < 2^32
+  if constexpr (F::ID == 0) {
+    return B::canon(r);
+  } else {
+    return B::canon(r >= 2 * F::P ? r - F::P : r);
+  }
+}
+
+// sum + D * x for D = +-2^-k and canonical x, without a Montgomery product.
+// With p = c * 2^S + 1, 2^-k = -c * 2^(S-k), so for x = hi * 2^k + lo:
+// x * 2^-k = hi - lo * c * 2^(S-k), and lo * c * 2^(S-k) < c * 2^S = p - 1.
+template <class F, int KSH, bool NEG>
+__device__ __forceinline__ uint32_t p2_add_pow2inv(uint32_t sum, uint32_t x) {
+  using B = Fp<F>;
+  constexpr uint32_t K = F::PC << (F::PS - KSH);
+  const uint32_t hi = x >> KSH;
+  const uint32_t m = (x & ((1u << KSH) - 1u)) * K;
+  // +: hi + p - m in [1, p + 2^(31-k));  -: m - hi + p in (p - 2^(31-k), 2p)
+  const uint32_t t = NEG ? (m - hi + F::P) : (hi + (F::P - m));
+  return B::add(sum, B::canon(t));
+}
+
+// Internal layer s_i = s_i * D_i + sum(s).  The sum is a tree: pairs of
+// canonical values fit 32 bits, the upper levels accumulate in 64 bits, one
+// reduction at the end.
+template <class F>
+__device__ __forceinline__ void p2_internal_v2(uint32_t s[16], const uint32_t* diag) {
+  using B = Fp<F>;
+  uint32_t pr[8];
 #pragma unroll
-  for (int i = 2; i < 16; i++) sum = B::add(sum, s[i]);
+  for (int i = 0; i < 8; i++) pr[i] = s[2 * i] + s[2 * i + 1];
+  const uint64_t q0 = (uint64_t)pr[0] + pr[1], q1 = (uint64_t)pr[2] + pr[3];
+  const uint64_t q2 = (uint64_t)pr[4] + pr[5], q3 = (uint64_t)pr[6] + pr[7];
+  const uint32_t sum = p2_reduce_sum<F>((q0 + q1) + (q2 + q3));
   // D[0..8] = -2, 1, 2, 1/2, 3, 4, -1/2, -3, -4 in both fields.
   s[0] = B::sub(sum, B::dbl(s[0]));
   s[1] = B::add(sum, s[1]);
@@ -89,32 +127,64 @@ __device__ __forceinline__ void p2_internal(uint32_t s[16]) {
   s[6] = B::sub(sum, B::half(s[6]));
   s[7] = B::sub(sum, B::add(B::dbl(s[7]), s[7]));
   s[8] = B::sub(sum, B::dbl(B::dbl(s[8])));
-#pragma unroll
-  for (int i = 9; i < 16; i++) s[i] = B::add(sum, B::mul(s[i], C.diag[i]));
+  // D[9..15]: KoalaBear 2^-8, 2^-3, 2^-24, -2^-8, -2^-3, -2^-4, -2^-24;
+  //           BabyBear  2^-8, 2^-2, 2^-3, 2^-27, -2^-8, -2^-4, -2^-27.
+  (void)diag;
+  if constexpr (F::ID == 0) {
+    s[9] = p2_add_pow2inv<F, 8, false>(sum, s[9]);
+    s[10] = p2_add_pow2inv<F, 3, false>(sum, s[10]);
+    s[11] = p2_add_pow2inv<F, 24, false>(sum, s[11]);
+    s[12] = p2_add_pow2inv<F, 8, true>(sum, s[12]);
+    s[13] = p2_add_pow2inv<F, 3, true>(sum, s[13]);
+    s[14] = p2_add_pow2inv<F, 4, true>(sum, s[14]);
+    s[15] = p2_add_pow2inv<F, 24, true>(sum, s[15]);
+  } else {
+    s[9] = p2_add_pow2inv<F, 8, false>(sum, s[9]);
+    s[10] = p2_add_pow2inv<F, 2, false>(sum, s[10]);
+    s[11] = p2_add_pow2inv<F, 3, false>(sum, s[11]);
+    s[12] = p2_add_pow2inv<F, 27, false>(sum, s[12]);
+    s[13] = p2_add_pow2inv<F, 8, true>(sum, s[13]);
+    s[14] = p2_add_pow2inv<F, 4, true>(sum, s[14]);
+    s[15] = p2_add_pow2inv<F, 27, true>(sum, s[15]);
+  }
 }
 
+template <class F>
+__device__ __forceinline__ void p2_full_round(uint32_t s[16], const uint32_t* rc) {
+  using B = Fp<F>;
+  uint32_t c[16];
+#pragma unroll
+  for (int j = 0; j < 16; j += 4) {
+    const uint4 v = *reinterpret_cast<const uint4*>(rc + j);
+    c[j] = v.x;
+    c[j + 1] = v.y;
+    c[j + 2] = v.z;
+    c[j + 3] = v.w;
+  }
+#pragma unroll
+  for (int j = 0; j < 16; j++) s[j] = p2_sbox<F>(B::add(s[j], c[j]));
+  p2_external<F>(s);
+}
+
+// Rounds run as loops (not unrolled) so the permutation's code stays small
+// enough for the instruction caches; each round reads its constants once.
 template <class F>
 __device__ __forceinline__ void p2_permute(uint32_t s[16]) {
   using B = Fp<F>;
   const P2Constants& C = c_p2[F::ID];
   p2_external<F>(s);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) p2_full_round<F>(s, C.ext[r]);
+  uint32_t diag[16];
 #pragma unroll
-  for (int r = 0; r < 4; r++) {
-#pragma unroll
-    for (int j = 0; j < 16; j++) s[j] = p2_sbox<F>(B::add(s[j], C.ext[r][j]));
-    p2_external<F>(s);
-  }
-#pragma unroll 4
+  for (int i = 9; i < 16; i++) diag[i] = C.diag[i];
+#pragma unroll 1
   for (int r = 0; r < F::ROUNDS_P; r++) {
     s[0] = p2_sbox<F>(B::add(s[0], C.inte[r]));
-    p2_internal<F>(s);
+    p2_internal_v2<F>(s, diag);
   }
-#pragma unroll
-  for (int r = 4; r < 8; r++) {
-#pragma unroll
-    for (int j = 0; j < 16; j++) s[j] = p2_sbox<F>(B::add(s[j], C.ext[r][j]));
-    p2_external<F>(s);
-  }
+#pragma unroll 1
+  for (int r = 4; r < 8; r++) p2_full_round<F>(s, C.ext[r]);
 }
 
 }  // namespace pico
