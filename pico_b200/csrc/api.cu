@@ -143,9 +143,11 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
   ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
   const uint32_t ns = (cfg && cfg->n_streams) ? cfg->n_streams : 8;
   for (uint32_t i = 0; i < ns; i++) {
-    cudaStream_t st;
+    cudaStream_t st, cst;
     if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
     ctx->streams.push_back(st);
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
+    ctx->copy_streams.push_back(cst);
   }
   // Constant tables for both fields.
   {
@@ -180,6 +182,10 @@ extern "C" pico_status pico_gpu_shutdown(pico_ctx* ctx) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
+  for (auto st : ctx->copy_streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
   for (int f = 0; f < 2; f++)
     if (ctx->tw[f]) cudaFree(ctx->tw[f]);
   delete ctx;
@@ -210,8 +216,9 @@ void unreserve(pico_ctx* ctx, uint64_t bytes) {
   ctx->reserved = bytes > ctx->reserved ? 0 : ctx->reserved - bytes;
   ctx->cv.notify_all();
 }
-cudaStream_t pick_stream(pico_ctx* ctx) {
+cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream) {
   uint32_t i = ctx->next_stream.fetch_add(1) % (uint32_t)ctx->streams.size();
+  if (copy_stream) *copy_stream = ctx->copy_streams[i];
   return ctx->streams[i];
 }
 TwiddleTables twiddles(pico_ctx* ctx, int field) {
@@ -311,13 +318,23 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   return PICO_OK;
 }
 
-// Enqueue a whole commit on `st`.  On success `c` holds the resident buffers
-// and `scratch` the buffers to free once the stream has passed this point.
-pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, pico_commit* c,
-                           std::vector<void*>& scratch, uint32_t* root_host) {
+// Enqueue a whole commit: compute on `st`, host -> device input copies on
+// `cst` (another stream, so copies overlap compute).  On success `c` holds
+// the resident buffers and `scratch` the buffers to free once `st` has passed
+// this point (the caller frees them on `st`, which waits for `cst`).
+//
+// Order of work.  The tree needs every height group's rows: the tallest
+// group as leaves, each shorter group as a digest injected at its level.
+// Host inputs are copied shortest group first, so the LDEs and row digests
+// of the short groups run while the tallest group is still in transit; the
+// tallest group's LDE, its leaf hashing and the compression levels come last.
+pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
+                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
   pico_status s;
   const int field = plan.field;
   const uint32_t n = (uint32_t)plan.mats.size();
+  const uint32_t G = (uint32_t)plan.groups.size();
+  const bool copy_in = !plan.input_device;
   c->ctx = ctx;
   c->field = field;
   c->log_max = plan.log_max;
@@ -332,34 +349,31 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   c->stats.permutations = plan.permutations;
   c->stats.leaf_permutations = plan.leaf_permutations;
   c->stats.lde_bytes = plan.extend ? 4 * (plan.cells + plan.lde_cells) : 0;
-  for (int e = 0; e < 5; e++)
+  for (int e = 0; e < 7; e++)
     if ((s = cuda_status(cudaEventCreate(&c->ev[e]), "event"))) return s;
   if ((s = cuda_status(cudaEventRecord(c->ev[0], st), "event"))) return s;
 
-  // Device copies of the inputs (or the caller's device pointers).
+  // ---- allocations (stream-ordered on st) ----
   std::vector<const uint32_t*> dev_in(n, nullptr);
+  std::vector<uint64_t> in_bytes(n, 0);
   for (uint32_t k = 0; k < n; k++) {
     const PlannedMat& m = plan.mats[k];
-    const uint64_t bytes = ((uint64_t)m.w << m.log_n) * 4;
-    if (plan.input_device || bytes == 0) {
+    in_bytes[k] = ((uint64_t)m.w << m.log_n) * 4;
+    if (!copy_in || in_bytes[k] == 0) {
       dev_in[k] = m.src;
     } else {
       void* d;
-      if ((s = alloc_async(&d, bytes, st))) return s;
+      if ((s = alloc_async(&d, in_bytes[k], st))) return s;
       if (plan.extend)
         scratch.push_back(d);
-      else {
+      else
         c->owns[m.input_idx] = true;
-      }
-      if ((s = cuda_status(cudaMemcpyAsync(d, m.src, bytes, cudaMemcpyHostToDevice, st), "input copy"))) return s;
       dev_in[k] = (const uint32_t*)d;
     }
   }
-
-  if ((s = cuda_status(cudaEventRecord(c->ev[1], st), "event"))) return s;
+  std::vector<LdeMat> hm(plan.extend ? n : 0);
   std::vector<const uint32_t*> leaves(n, nullptr);  // what the tree hashes, per planned matrix
   if (plan.extend) {
-    std::vector<LdeMat> hm(n);
     const uint32_t nb = 1u << plan.log_b;
     void* pw;  // one allocation for all (matrix, coset) power tables
     if ((s = alloc_async(&pw, (uint64_t)n * nb * kPwWords * 4, st))) return s;
@@ -393,13 +407,6 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
         L.t2 = (uint32_t*)t2;
       }
     }
-    const TwiddleTables tw = twiddles(ctx, field);
-    if (plan.plain) {
-      for (uint32_t k = 0; k < n; k++)
-        if ((s = cuda_status(launch_lde(field, &hm[k], 1, tw, st, &c->stats.launches), "LDE launch"))) return s;
-    } else {
-      if ((s = cuda_status(launch_lde(field, hm.data(), n, tw, st, &c->stats.launches), "LDE launch"))) return s;
-    }
   } else {
     for (uint32_t k = 0; k < n; k++) {
       const PlannedMat& m = plan.mats[k];
@@ -409,14 +416,67 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       c->width[m.input_idx] = m.w;
     }
   }
-
-  if ((s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) return s;
-  // Merkle tree over all (extended) matrices.
   const uint32_t log_max = plan.log_max;
-  const uint64_t total_digests = (2ull << log_max) - 1;
   void* layers;
-  if ((s = alloc_async(&layers, total_digests * 32, st))) return s;
+  if ((s = alloc_async(&layers, ((2ull << log_max) - 1) * 32, st))) return s;
   c->layers = (uint32_t*)layers;
+  // digests of the rows of every shorter height group, injected at its level
+  std::vector<uint32_t*> inj(G, nullptr);
+  {
+    uint64_t words = 0;
+    for (uint32_t g = 1; g < G; g++) words += 8ull << plan.mats[plan.groups[g].first].log_N;
+    if (words) {
+      void* d;
+      if ((s = alloc_async(&d, words * 4, st))) return s;
+      scratch.push_back(d);
+      uint64_t off = 0;
+      for (uint32_t g = 1; g < G; g++) {
+        inj[g] = (uint32_t*)d + off;
+        off += 8ull << plan.mats[plan.groups[g].first].log_N;
+      }
+    }
+  }
+
+  // ---- host -> device copies on cst, shortest group first ----
+  std::vector<cudaEvent_t> arrived(G, nullptr);
+  auto destroy_events = [&]() {
+    for (auto e : arrived)
+      if (e) cudaEventDestroy(e);  // released once the device has passed them
+  };
+  if ((s = cuda_status(cudaEventRecord(c->ev[5], st), "event"))) return s;
+  if (copy_in) {
+    if ((s = cuda_status(cudaStreamWaitEvent(cst, c->ev[5], 0), "copy stream wait"))) return s;
+    for (uint32_t gi = G; gi-- > 0;) {
+      for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) {
+        if (!in_bytes[k]) continue;
+        if ((s = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(dev_in[k]), plan.mats[k].src, in_bytes[k],
+                                             cudaMemcpyHostToDevice, cst),
+                             "input copy"))) {
+          destroy_events();
+          return s;
+        }
+      }
+      cudaEvent_t e;
+      if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) {
+        destroy_events();
+        return s;
+      }
+      arrived[gi] = e;
+      if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) {
+        destroy_events();
+        return s;
+      }
+    }
+    if ((s = cuda_status(cudaEventRecord(c->ev[6], cst), "event"))) {
+      destroy_events();
+      return s;
+    }
+  } else {
+    if ((s = cuda_status(cudaEventRecord(c->ev[6], st), "event"))) return s;
+  }
+
+  // ---- compute on st ----
+  const TwiddleTables tw = twiddles(ctx, field);
   auto make_group = [&](uint32_t gi, RowGroup& g) {
     memset(&g, 0, sizeof g);
     const auto& gr = plan.groups[gi];
@@ -427,6 +487,52 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       g.total_width += plan.mats[k].w;
     }
   };
+  auto lde_group = [&](uint32_t first, uint32_t last) -> pico_status {
+    if (!plan.extend || first == last) return PICO_OK;
+    if (plan.plain) {
+      for (uint32_t k = first; k < last; k++)
+        if (pico_status r = cuda_status(launch_lde(field, &hm[k], 1, tw, st, &c->stats.launches), "LDE launch"))
+          return r;
+      return PICO_OK;
+    }
+    return cuda_status(launch_lde(field, &hm[first], last - first, tw, st, &c->stats.launches), "LDE launch");
+  };
+  auto digest_group = [&](uint32_t gi) -> pico_status {
+    RowGroup g;
+    make_group(gi, g);
+    pico_status r = cuda_status(
+        launch_hash_rows(field, g, 1ull << plan.mats[plan.groups[gi].first].log_N, inj[gi], st), "row hashing");
+    c->stats.launches += 1;
+    return r;
+  };
+  if (copy_in) {
+    // per group as its inputs arrive: LDE, then (below the tallest) row digests
+    for (uint32_t gi = G; gi-- > 0;) {
+      if ((s = cuda_status(cudaStreamWaitEvent(st, arrived[gi], 0), "wait for inputs"))) {
+        destroy_events();
+        return s;
+      }
+      if ((s = lde_group(plan.groups[gi].first, plan.groups[gi].second))) {
+        destroy_events();
+        return s;
+      }
+      if (gi > 0 && (s = digest_group(gi))) {
+        destroy_events();
+        return s;
+      }
+    }
+    destroy_events();
+    if ((s = cuda_status(cudaEventRecord(c->ev[1], st), "event"))) return s;
+    if ((s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) return s;
+  } else {
+    if ((s = lde_group(0, n))) return s;
+    if ((s = cuda_status(cudaEventRecord(c->ev[1], st), "event"))) return s;
+    for (uint32_t gi = 1; gi < G; gi++)
+      if ((s = digest_group(gi))) return s;
+    if ((s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) return s;
+  }
+
+  // leaves: rows of the tallest group
   RowGroup g0;
   make_group(0, g0);
   uint32_t* layer = c->layers;
@@ -437,14 +543,9 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   for (uint32_t lvl = 1; lvl <= log_max; lvl++) {
     const uint64_t len = 1ull << (log_max - lvl);
     uint32_t* next = layer + (2 * len) * 8;
-    RowGroup gi;
-    const RowGroup* inj = nullptr;
-    if (next_group < plan.groups.size() && plan.mats[plan.groups[next_group].first].log_N == log_max - lvl) {
-      make_group(next_group, gi);
-      inj = &gi;
-      next_group++;
-    }
-    if ((s = cuda_status(launch_compress(field, layer, next, len, inj, st), "compression"))) return s;
+    const uint32_t* d = nullptr;
+    if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - lvl) d = inj[next_group++];
+    if ((s = cuda_status(launch_compress(field, layer, next, len, d, st), "compression"))) return s;
     c->stats.launches += 1;
     layer = next;
   }
@@ -455,19 +556,25 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
 }
 
 // Fill c->stats timings from its events (blocks until the commit finished).
+// Events: 0 start, 1 LDEs done, 2 injected-row digests done, 3 leaves done,
+// 4 root ready (all on the compute stream); 5 copies may start, 6 copies
+// done (copy stream).  With host inputs the LDE span includes waiting for
+// the copies it overlaps.
 pico_status finish_stats(pico_commit* c) {
   if (!c->ev[4]) return PICO_OK;
   pico_status s;
   if ((s = cuda_status(cudaEventSynchronize(c->ev[4]), "commit events"))) return s;
-  float t[4];
+  if ((s = cuda_status(cudaEventSynchronize(c->ev[6]), "commit events"))) return s;
+  float t[5];
   for (int i = 0; i < 4; i++)
     if ((s = cuda_status(cudaEventElapsedTime(&t[i], c->ev[i], c->ev[i + 1]), "event timing"))) return s;
-  c->stats.h2d_ms = t[0];
-  c->stats.lde_ms = t[1];
+  if ((s = cuda_status(cudaEventElapsedTime(&t[4], c->ev[5], c->ev[6]), "event timing"))) return s;
+  c->stats.lde_ms = t[0];
   c->stats.leaves_ms = t[2];
-  c->stats.tree_ms = t[3];
+  c->stats.tree_ms = (double)t[1] + t[3];
+  c->stats.h2d_ms = t[4];
   c->stats.total_ms = (double)t[0] + t[1] + t[2] + t[3];
-  for (int e = 0; e < 5; e++) {
+  for (int e = 0; e < 7; e++) {
     cudaEventDestroy(c->ev[e]);
     c->ev[e] = nullptr;
   }
@@ -485,7 +592,7 @@ void free_commit_buffers(pico_commit* c, cudaStream_t st) {
 }  // namespace pico
 
 pico_commit::~pico_commit() {
-  for (int e = 0; e < 5; e++)
+  for (int e = 0; e < 7; e++)
     if (ev[e]) cudaEventDestroy(ev[e]);
 }
 
@@ -512,11 +619,14 @@ static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_mat
     return PICO_ERR_OUT_OF_MEMORY;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t cst;
+  cudaStream_t st = pick_stream(ctx, &cst);
   auto c = std::make_unique<pico_commit>();
   std::vector<void*> scratch;
   uint32_t root_h[8];
-  s = enqueue_commit(ctx, plan, st, c.get(), scratch, root_h);
+  s = enqueue_commit(ctx, plan, st, cst, c.get(), scratch, root_h);
+  // On failure the copy stream may still be writing into scratch buffers.
+  if (s) cudaStreamSynchronize(cst);
   for (void* p : scratch) cudaFreeAsync(p, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "commit");
   if (!s) s = s2;

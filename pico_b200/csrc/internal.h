@@ -30,10 +30,10 @@ cudaError_t upload_p2_constants(int field, const uint32_t ext[8][16], const uint
                                 const uint32_t diag[16]);
 cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st);
 cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st);
-// next[i] = compress(prev[2i], prev[2i+1]); if inject != null:
-// next[i] = compress(next[i], hash(inject rows i)).
+// next[i] = compress(prev[2i], prev[2i+1]); if inj_digests != null:
+// next[i] = compress(next[i], inj_digests[i]) (8 words per digest).
 cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,
-                            const RowGroup* inject, cudaStream_t st);
+                            const uint32_t* inj_digests, cudaStream_t st);
 
 // --- FRI kernels (p2_kernels.cu) ----------------------------------------
 // Device-side duplex challenger state, Monty form.

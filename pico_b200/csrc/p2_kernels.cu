@@ -83,9 +83,13 @@ __global__ void __launch_bounds__(256) k_hash_rows(const __grid_constant__ RowGr
   store_digest(out + 8 * r, s);
 }
 
+// next[i] = compress(prev[2i], prev[2i+1]); where a matrix height meets this
+// level, next[i] = compress(next[i], inj[i]) with inj[i] the digest of the
+// concatenated rows i of those matrices (TruncatedPermutation, hash.rs:89-94;
+// injection order of the verifier, fri.rs:389-436).
 template <class F>
 __global__ void __launch_bounds__(256)
-    k_compress(const uint32_t* prev, uint32_t* next, uint64_t n, const __grid_constant__ RowGroup g) {
+    k_compress(const uint32_t* prev, uint32_t* next, uint64_t n, const uint32_t* inj) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t s[16];
@@ -99,13 +103,17 @@ __global__ void __launch_bounds__(256)
     s[4 * k + 3] = v.w;
   }
   p2_permute<F>(s);
-  if (g.n_segs) {
-    uint32_t h[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) h[k] = 0;
-    hash_row<F>(g, i, h);
-#pragma unroll
-    for (int k = 0; k < 8; k++) s[8 + k] = h[k];
+  if (inj) {
+    const uint4* q = reinterpret_cast<const uint4*>(inj + 8 * i);
+    const uint4 a = __ldg(q), b = __ldg(q + 1);
+    s[8] = a.x;
+    s[9] = a.y;
+    s[10] = a.z;
+    s[11] = a.w;
+    s[12] = b.x;
+    s[13] = b.y;
+    s[14] = b.z;
+    s[15] = b.w;
     p2_permute<F>(s);
   }
   store_digest(next + 8 * i, s);
@@ -133,14 +141,12 @@ cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32
 }
 
 cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,
-                            const RowGroup* inject, cudaStream_t st) {
+                            const uint32_t* inj_digests, cudaStream_t st) {
   if (n_next == 0) return cudaSuccess;
-  RowGroup none{};
-  const RowGroup& g = inject ? *inject : none;
   if (field == 0)
-    k_compress<KoalaBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, g);
+    k_compress<KoalaBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, inj_digests);
   else
-    k_compress<BabyBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, g);
+    k_compress<BabyBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, inj_digests);
   return cudaGetLastError();
 }
 

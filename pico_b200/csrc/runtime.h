@@ -61,10 +61,10 @@ struct Server;  // serving.h
 
 bool try_reserve(pico_ctx* ctx, uint64_t bytes);
 void unreserve(pico_ctx* ctx, uint64_t bytes);
-cudaStream_t pick_stream(pico_ctx* ctx);
+cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr);
 TwiddleTables twiddles(pico_ctx* ctx, int field);
-pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, pico_commit* c,
-                           std::vector<void*>& scratch, uint32_t* root_host);
+pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
+                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
 void free_commit_buffers(pico_commit* c, cudaStream_t st);
 pico_status finish_stats(pico_commit* c);
 
@@ -78,6 +78,7 @@ struct pico_ctx {
   std::mutex mu;               // guards budget accounting
   std::condition_variable cv;  // signalled whenever reserved memory is returned
   std::vector<cudaStream_t> streams;
+  std::vector<cudaStream_t> copy_streams;  // paired with streams[i]: host -> device input copies
   std::atomic<uint32_t> next_stream{0};
   uint32_t* tw[2] = {nullptr, nullptr};  // per-field twiddle tables (lo | hi)
   pico::Server* server = nullptr;
@@ -97,8 +98,8 @@ struct pico_commit {
   uint32_t* layers = nullptr;     // all digest layers, leaves first
   uint64_t bytes_resident = 0;
   uint32_t root[8] = {0};
-  // events: start, inputs copied, LDE done, leaves done, tree done
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // events (see finish_stats): compute-stream phases 0..4, copy stream 5..6
+  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   pico_commit_stats stats{};
   ~pico_commit();
 };

@@ -97,7 +97,8 @@ static void launch_request(Server* sv, pico_request* r) {
   pico_ctx* ctx = sv->ctx;
   cudaStream_t st = ctx->streams[r->slot];
   r->commit = new pico_commit();
-  pico_status s = enqueue_commit(ctx, r->plan, st, r->commit, r->scratch, r->root_pinned);
+  pico_status s = enqueue_commit(ctx, r->plan, st, ctx->copy_streams[r->slot], r->commit, r->scratch, r->root_pinned);
+  if (s) cudaStreamSynchronize(ctx->copy_streams[r->slot]);  // copies may still target scratch
   for (void* p : r->scratch) cudaFreeAsync(p, st);
   r->scratch.clear();
   if (s == PICO_OK) s = cuda_status(cudaLaunchHostFunc(st, on_request_done, r), "completion callback");
