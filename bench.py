@@ -56,8 +56,17 @@ def uneven_kb_shapes(seed: int = 2, n: int = 32, target_log: int = 30, lo: int =
     raise RuntimeError("could not draw the workload")
 
 
+def recursion_bb_shapes(seed: int = 3, n: int = 48, lo: int = 8, hi: int = 20):
+    """48 BabyBear traces: log2 heights uniform on [8, 20], widths uniform on [4, 600]."""
+    rng = np.random.default_rng(seed)
+    logh = rng.integers(lo, hi + 1, size=n)
+    w = rng.integers(4, 601, size=n)
+    return [(int(a), int(b)) for a, b in zip(logh, w)]
+
+
 WORKLOADS = {
     "uneven-kb-2^30": dict(field=0, log_blowup=1, shapes=lambda: uneven_kb_shapes(), seed=2),
+    "recursion-bb-48": dict(field=1, log_blowup=2, shapes=lambda: recursion_bb_shapes(), seed=3),
     "single-kb-2^16x64": dict(field=0, log_blowup=1, shapes=lambda: [(16, 64)], seed=1),
     # same shape distribution scaled to 2^25 cells (heights 2^6..2^18): for profiler captures
     "uneven-kb-2^25": dict(field=0, log_blowup=1, shapes=lambda: uneven_kb_shapes(target_log=25, lo=6, hi=18),
@@ -350,13 +359,183 @@ def run_gpu(args, rank, world, local):
     return result, shapes, field, b
 
 
+# ---------------------------------------------------------------- FRI leg
+def run_fri(args):
+    """FRI commit phase on a device-resident KoalaBear EF4 codeword of 2^23
+    evaluations (a degree < 2^22 random polynomial, coset LDE with blowup 2):
+    per round Poseidon2 Merkle commit of the (len/2) x 2 extension matrix,
+    on-device challenger, arity-2 fold; all layers stay resident.  Two
+    stopping rules: the reference's (fold to 2^log_blowup, single final
+    element) and 2^4 final coefficients."""
+    import torch
+
+    from pico_b200 import GpuContext, Radix2DitParallel, TwoAdicFriPcs
+    from pico_b200 import fields as F
+
+    f, log_trace, b = 0, 22, 1
+    dev = torch.device("cuda", 0)
+    ctx = GpuContext(0)
+    base = F.random_matrix_torch(f, log_trace, 4, 4000, dev)
+    cw = torch.empty((1 << (log_trace + b), 4), dtype=torch.int32, device=dev)
+    Radix2DitParallel(ctx, f).coset_lde_batch_bitrev(base, b, F.lde_shift(f), out=cw)
+    torch.cuda.synchronize()
+    pcs = TwoAdicFriPcs(ctx, f, b)
+    out = {}
+    for name, lf in (("final_1", 0), ("final_16", 4)):
+        for _ in range(args.warmup):
+            pcs.fri_commit_phase(cw, log_final_len=lf)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            res = pcs.fri_commit_phase(cw, log_final_len=lf)
+        torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out[name] = {"ms": ms, "rounds": res.rounds, "elements_per_s": (1 << (log_trace + b)) / (ms / 1e3)}
+    ctx.close()
+    return {
+        "metric": "FRI commit-phase codeword elements/sec (EF4, arity 2, Poseidon2 layer commits)",
+        "value": out["final_1"]["elements_per_s"], "unit": "elements/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out["final_1"]["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (KoalaBear EF4)", "data": "synthetic: random degree < 2^22 EF4 polynomial",
+        "config": {"workload": "fri-kb-2^23", "log_n": log_trace + b, "log_blowup": b}, "modes": out,
+    }
+
+
+# ---------------------------------------------------------------- serving leg
+def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30):
+    """Requests of 1..40 matrices, log2 heights uniform on [12, 21], widths
+    uniform on [16, 512]; 70% KoalaBear / 30% BabyBear; log_blowup 1 or 2.
+    A request is cut to its first matrices totalling at most max_cells trace
+    cells, so that one request (with its blowup-4 LDEs and scratch) fits HBM."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(n_req):
+        k = int(rng.integers(1, 41))
+        f = 0 if rng.random() < 0.7 else 1
+        b = int(rng.integers(1, 3))
+        shapes = [(int(rng.integers(12, 22)), int(rng.integers(16, 513))) for _ in range(k)]
+        kept, tot = [], 0
+        for lh, w in shapes:
+            if kept and tot + (w << lh) > max_cells:
+                break
+            kept.append((lh, w))
+            tot += w << lh
+        reqs.append((f, b, kept))
+    return reqs
+
+
+def run_serving(args):
+    """Poisson arrivals of commit requests into the serving queue (admission
+    by free HBM, concurrent streams), against the same requests committed one
+    at a time (batched form, and plain one-matrix-per-launch form).  Inputs
+    are views into a device-resident pool of seeded field elements."""
+    import threading as th
+
+    import torch
+
+    from pico_b200 import CommitServer, GpuContext, TwoAdicDomain, TwoAdicFriPcs
+    from pico_b200 import fields as F
+
+    dev = torch.device("cuda", 0)
+    reqs = serving_requests(args.requests)
+    pool_cells = 1 << 30
+    pools = {f: F.random_matrix_torch(f, 30, 1, 5000 + f, dev).reshape(-1) for f in (0, 1)}
+
+    def views(f, shapes, salt):
+        rng = np.random.default_rng(salt)
+        out = []
+        for lh, w in shapes:
+            cells = w << lh
+            if cells > pool_cells:
+                raise ValueError("matrix larger than the pool")
+            off = int(rng.integers(0, (pool_cells - cells) // 4 + 1)) * 4
+            out.append(pools[f][off:off + cells].view(1 << lh, w))
+        return out
+
+    mats = [views(f, shapes, 7 * i + 1) for i, (f, b, shapes) in enumerate(reqs)]
+    cells = [sum(w << lh for lh, w in shapes) for (_, _, shapes) in reqs]
+    total_cells = sum(cells)
+    ctx = GpuContext(0, n_streams=8)
+
+    # one at a time: batched and plain forms
+    def sequential(plain):
+        lat = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for (f, b, shapes), m in zip(reqs, mats):
+            t = time.perf_counter()
+            pcs = TwoAdicFriPcs(ctx, f, b)
+            pcs.commit([(TwoAdicDomain(lh), x) for (lh, _), x in zip(shapes, m)], plain=plain, keep=False)
+            lat.append(time.perf_counter() - t)
+        return time.perf_counter() - t0, lat
+
+    warm = min(3, len(reqs))
+    for (f, b, shapes), m in list(zip(reqs, mats))[:warm]:
+        TwoAdicFriPcs(ctx, f, b).commit([(TwoAdicDomain(lh), x) for (lh, _), x in zip(shapes, m)], keep=False)
+    seq_s, seq_lat = sequential(False)
+    plain_s, plain_lat = sequential(True)
+    capacity = total_cells / seq_s
+    rate = args.load * capacity / (total_cells / len(reqs))  # requests per second
+    rng = np.random.default_rng(55)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+
+    server = CommitServer(ctx)
+    handles = [None] * len(reqs)
+    lat = [None] * len(reqs)
+    t_submit = [0.0] * len(reqs)
+    t0 = time.perf_counter()
+
+    def waiter():
+        for i in range(len(reqs)):
+            while handles[i] is None:
+                time.sleep(0.0002)
+            handles[i].wait(keep=False)
+            q_us, run_us = handles[i].times()
+            lat[i] = (q_us + run_us) / 1e6
+            handles[i].free()
+
+    wt = th.Thread(target=waiter)
+    wt.start()
+    for i, ((f, b, shapes), m) in enumerate(zip(reqs, mats)):
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        t_submit[i] = time.perf_counter() - t0
+        handles[i] = server.submit(f, m, b)
+    wt.join()
+    served_s = time.perf_counter() - t0
+    ctx.close()
+
+    def pct(x, q):
+        return float(np.percentile(np.array(x) * 1e3, q))
+
+    return {
+        "metric": "served commit throughput (trace cells/sec) with p50/p99 latency",
+        "value": total_cells / served_s, "unit": "cells/s", "n_gpus": 1, "steps": len(reqs), "warmup": warm,
+        "ms_per_step": served_s * 1e3 / len(reqs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic: views into a seeded device pool",
+        "config": {"workload": "serving", "requests": len(reqs), "offered_load": args.load,
+                   "poisson_rate_per_s": rate, "total_cells": total_cells},
+        "served": {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "cells_per_s": total_cells / served_s},
+        "one_at_a_time_batched": {"p50_ms": pct(seq_lat, 50), "p99_ms": pct(seq_lat, 99),
+                                  "cells_per_s": total_cells / seq_s},
+        "one_at_a_time_plain": {"p50_ms": pct(plain_lat, 50), "p99_ms": pct(plain_lat, 99),
+                                "cells_per_s": total_cells / plain_s},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=list(WORKLOADS), default="uneven-kb-2^30")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving"], default="uneven-kb-2^30")
+    ap.add_argument("--requests", type=int, default=60, help="serving: number of requests")
+    ap.add_argument("--load", type=float, default=0.8, help="serving: offered load vs one-at-a-time capacity")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
@@ -364,6 +543,11 @@ def main():
     args = ap.parse_args()
 
     rank, world, local = dist_setup(args.gpus)
+    if args.workload in ("fri-kb-2^23", "serving"):
+        if rank == 0:
+            res = run_fri(args) if args.workload == "fri-kb-2^23" else run_serving(args)
+            print(json.dumps(res), flush=True)
+        return
     wl = WORKLOADS[args.workload]
 
     if args.impl == "reference":

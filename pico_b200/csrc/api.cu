@@ -149,6 +149,11 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
     if ((s = cuda_status(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
     ctx->copy_streams.push_back(cst);
   }
+  for (uint32_t i = 0; i < 4; i++) {
+    cudaStream_t st;
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
+    ctx->aux_streams.push_back(st);
+  }
   // Constant tables for both fields.
   {
     uint32_t ext[8][16], inte[24] = {0}, diag[16];
@@ -186,6 +191,10 @@ extern "C" pico_status pico_gpu_shutdown(pico_ctx* ctx) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
+  for (auto st : ctx->aux_streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
   for (int f = 0; f < 2; f++)
     if (ctx->tw[f]) cudaFree(ctx->tw[f]);
   delete ctx;
@@ -216,6 +225,13 @@ void unreserve(pico_ctx* ctx, uint64_t bytes) {
   ctx->reserved = bytes > ctx->reserved ? 0 : ctx->reserved - bytes;
   ctx->cv.notify_all();
 }
+// Streams for read-backs and releases of finished work: they never carry
+// long compute, so synchronising them cannot wait on another request.
+cudaStream_t aux_stream(pico_ctx* ctx) {
+  uint32_t i = ctx->next_aux.fetch_add(1) % (uint32_t)ctx->aux_streams.size();
+  return ctx->aux_streams[i];
+}
+
 cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream) {
   uint32_t i = ctx->next_stream.fetch_add(1) % (uint32_t)ctx->streams.size();
   if (copy_stream) *copy_stream = ctx->copy_streams[i];
@@ -688,7 +704,7 @@ extern "C" pico_status pico_gpu_release(pico_ctx* ctx, pico_commit* c) {
     return PICO_ERR_INVALID_ARG;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t st = aux_stream(ctx);
   free_commit_buffers(c, st);
   pico_status s = cuda_status(cudaStreamSynchronize(st), "release");
   unreserve(ctx, c->bytes_resident);
@@ -723,7 +739,7 @@ extern "C" pico_status pico_gpu_lde_rows(pico_ctx* ctx, const pico_commit* c, ui
   const uint64_t w = c->width[mat_idx];
   const size_t bytes = (row_end - row_begin) * w * 4;
   if (!bytes) return PICO_OK;
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t st = aux_stream(ctx);
   pico_status s = cuda_status(cudaMemcpyAsync(out, c->lde[mat_idx] + row_begin * w, bytes,
                                               (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice
                                                                            : cudaMemcpyDeviceToHost,
@@ -743,7 +759,7 @@ extern "C" pico_status pico_gpu_digest_layer(pico_ctx* ctx, const pico_commit* c
   uint64_t off = 0;
   for (uint32_t l = 0; l < level; l++) off += 1ull << (c->log_max - l);
   const size_t bytes = (1ull << (c->log_max - level)) * 32;
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t st = aux_stream(ctx);
   pico_status s = cuda_status(
       cudaMemcpyAsync(out, c->layers + off * 8, bytes,
                       (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st),
@@ -759,7 +775,7 @@ extern "C" pico_status pico_gpu_open_batch(pico_ctx* ctx, const pico_commit* c, 
     return PICO_ERR_INVALID_ARG;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t st = aux_stream(ctx);
   pico_status s;
   if (rows_out) {
     uint64_t off = 0;

@@ -207,7 +207,7 @@ extern "C" pico_status pico_gpu_fri_release(pico_ctx* ctx, pico_fri* f) {
     return PICO_ERR_INVALID_ARG;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t st = aux_stream(ctx);
   for (auto p : f->codewords) cudaFreeAsync(p, st);
   for (auto p : f->trees) cudaFreeAsync(p, st);
   pico_status s = cuda_status(cudaStreamSynchronize(st), "fri_release");
@@ -223,7 +223,7 @@ extern "C" pico_status pico_gpu_fri_layer(pico_ctx* ctx, const pico_fri* f, uint
     return PICO_ERR_INVALID_ARG;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  cudaStream_t st = aux_stream(ctx);
   pico_status s = cuda_status(cudaMemcpyAsync(out, f->codewords[round], 16ull << (f->log_n - round),
                                               (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice
                                                                            : cudaMemcpyDeviceToHost,

@@ -62,6 +62,7 @@ struct Server;  // serving.h
 bool try_reserve(pico_ctx* ctx, uint64_t bytes);
 void unreserve(pico_ctx* ctx, uint64_t bytes);
 cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr);
+cudaStream_t aux_stream(pico_ctx* ctx);
 TwiddleTables twiddles(pico_ctx* ctx, int field);
 pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
                            pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
@@ -80,6 +81,8 @@ struct pico_ctx {
   std::vector<cudaStream_t> streams;
   std::vector<cudaStream_t> copy_streams;  // paired with streams[i]: host -> device input copies
   std::atomic<uint32_t> next_stream{0};
+  std::vector<cudaStream_t> aux_streams;  // read-backs and releases of finished work
+  std::atomic<uint32_t> next_aux{0};
   uint32_t* tw[2] = {nullptr, nullptr};  // per-field twiddle tables (lo | hi)
   pico::Server* server = nullptr;
   ~pico_ctx();
