@@ -148,6 +148,8 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
     ctx->streams.push_back(st);
     if ((s = cuda_status(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
     ctx->copy_streams.push_back(cst);
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
+    ctx->lde_streams.push_back(cst);
   }
   for (uint32_t i = 0; i < 4; i++) {
     cudaStream_t st;
@@ -188,6 +190,10 @@ extern "C" pico_status pico_gpu_shutdown(pico_ctx* ctx) {
     cudaStreamDestroy(st);
   }
   for (auto st : ctx->copy_streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (auto st : ctx->lde_streams) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
@@ -232,9 +238,10 @@ cudaStream_t aux_stream(pico_ctx* ctx) {
   return ctx->aux_streams[i];
 }
 
-cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream) {
+cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream, cudaStream_t* lde_stream) {
   uint32_t i = ctx->next_stream.fetch_add(1) % (uint32_t)ctx->streams.size();
   if (copy_stream) *copy_stream = ctx->copy_streams[i];
+  if (lde_stream) *lde_stream = ctx->lde_streams[i];
   return ctx->streams[i];
 }
 TwiddleTables twiddles(pico_ctx* ctx, int field) {
@@ -334,8 +341,8 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   return PICO_OK;
 }
 
-// Enqueue a whole commit: compute on `st`, host -> device input copies on
-// `cst` (another stream, so copies overlap compute).  On success `c` holds
+// Enqueue a whole commit: Poseidon2 on `st`, LDEs on `lst`, host -> device
+// input copies on `cst` (three streams, so copies, LDEs and hashing overlap).  On success `c` holds
 // the resident buffers and `scratch` the buffers to free once `st` has passed
 // this point (the caller frees them on `st`, which waits for `cst`).
 //
@@ -345,7 +352,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
 // of the short groups run while the tallest group is still in transit; the
 // tallest group's LDE, its leaf hashing and the compression levels come last.
 pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
-                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
+                           cudaStream_t lst, pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
   pico_status s;
   const int field = plan.field;
   const uint32_t n = (uint32_t)plan.mats.size();
@@ -491,7 +498,10 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     if ((s = cuda_status(cudaEventRecord(c->ev[6], st), "event"))) return s;
   }
 
-  // ---- compute on st ----
+  // ---- compute: LDEs on lst, Poseidon2 on st, pipelined per height group ----
+  // The LDE of one group runs while the previous group's rows are hashed:
+  // the LDE kernels stall on memory latency while hashing saturates the
+  // integer pipes, so the two share the SMs well.
   const TwiddleTables tw = twiddles(ctx, field);
   auto make_group = [&](uint32_t gi, RowGroup& g) {
     memset(&g, 0, sizeof g);
@@ -507,54 +517,70 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     if (!plan.extend || first == last) return PICO_OK;
     if (plan.plain) {
       for (uint32_t k = first; k < last; k++)
-        if (pico_status r = cuda_status(launch_lde(field, &hm[k], 1, tw, st, &c->stats.launches), "LDE launch"))
+        if (pico_status r = cuda_status(launch_lde(field, &hm[k], 1, tw, lst, &c->stats.launches), "LDE launch"))
           return r;
       return PICO_OK;
     }
-    return cuda_status(launch_lde(field, &hm[first], last - first, tw, st, &c->stats.launches), "LDE launch");
+    return cuda_status(launch_lde(field, &hm[first], last - first, tw, lst, &c->stats.launches), "LDE launch");
   };
-  auto digest_group = [&](uint32_t gi) -> pico_status {
+  // Device inputs: tallest group first (its leaf hashing is the longest job).
+  // Host inputs: the order the copies arrive in (shortest first).
+  std::vector<uint32_t> order;
+  for (uint32_t i = 0; i < G; i++) order.push_back(copy_in ? G - 1 - i : i);
+  std::vector<cudaEvent_t> lde_done(G, nullptr);
+  auto destroy_all = [&]() {
+    destroy_events();
+    for (auto e : lde_done)
+      if (e) cudaEventDestroy(e);
+  };
+  if ((s = cuda_status(cudaStreamWaitEvent(lst, c->ev[5], 0), "LDE stream wait"))) {
+    destroy_all();
+    return s;
+  }
+  for (uint32_t gi : order) {
+    if (copy_in && (s = cuda_status(cudaStreamWaitEvent(lst, arrived[gi], 0), "wait for inputs"))) {
+      destroy_all();
+      return s;
+    }
+    if ((s = lde_group(plan.groups[gi].first, plan.groups[gi].second))) {
+      destroy_all();
+      return s;
+    }
+    if ((s = cuda_status(cudaEventCreateWithFlags(&lde_done[gi], cudaEventDisableTiming), "event")) ||
+        (s = cuda_status(cudaEventRecord(lde_done[gi], lst), "event"))) {
+      destroy_all();
+      return s;
+    }
+  }
+  if ((s = cuda_status(cudaEventRecord(c->ev[1], lst), "event"))) {
+    destroy_all();
+    return s;
+  }
+  uint32_t* layer = c->layers;
+  for (uint32_t gi : order) {
+    if ((s = cuda_status(cudaStreamWaitEvent(st, lde_done[gi], 0), "wait for LDE"))) {
+      destroy_all();
+      return s;
+    }
     RowGroup g;
     make_group(gi, g);
-    pico_status r = cuda_status(
-        launch_hash_rows(field, g, 1ull << plan.mats[plan.groups[gi].first].log_N, inj[gi], st), "row hashing");
-    c->stats.launches += 1;
-    return r;
-  };
-  if (copy_in) {
-    // per group as its inputs arrive: LDE, then (below the tallest) row digests
-    for (uint32_t gi = G; gi-- > 0;) {
-      if ((s = cuda_status(cudaStreamWaitEvent(st, arrived[gi], 0), "wait for inputs"))) {
-        destroy_events();
-        return s;
-      }
-      if ((s = lde_group(plan.groups[gi].first, plan.groups[gi].second))) {
-        destroy_events();
-        return s;
-      }
-      if (gi > 0 && (s = digest_group(gi))) {
-        destroy_events();
-        return s;
-      }
+    if (gi == 0 && (s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) {
+      destroy_all();
+      return s;
     }
-    destroy_events();
-    if ((s = cuda_status(cudaEventRecord(c->ev[1], st), "event"))) return s;
-    if ((s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) return s;
-  } else {
-    if ((s = lde_group(0, n))) return s;
-    if ((s = cuda_status(cudaEventRecord(c->ev[1], st), "event"))) return s;
-    for (uint32_t gi = 1; gi < G; gi++)
-      if ((s = digest_group(gi))) return s;
-    if ((s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) return s;
+    s = cuda_status(launch_hash_rows(field, g, 1ull << plan.mats[plan.groups[gi].first].log_N,
+                                     gi == 0 ? layer : inj[gi], st),
+                    gi == 0 ? "leaf hashing" : "row hashing");
+    c->stats.launches += 1;
+    if (!s && gi == 0) s = cuda_status(cudaEventRecord(c->ev[3], st), "event");
+    if (s) {
+      destroy_all();
+      return s;
+    }
   }
-
-  // leaves: rows of the tallest group
-  RowGroup g0;
-  make_group(0, g0);
-  uint32_t* layer = c->layers;
-  if ((s = cuda_status(launch_hash_rows(field, g0, 1ull << log_max, layer, st), "leaf hashing"))) return s;
-  c->stats.launches += 1;
-  if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;
+  destroy_all();
+  // the tree below needs every LDE; the last lde_done wait covered all of them
+  // (the LDE stream runs the groups in order)
   uint32_t next_group = 1;
   for (uint32_t lvl = 1; lvl <= log_max; lvl++) {
     const uint64_t len = 1ull << (log_max - lvl);
@@ -572,24 +598,27 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
 }
 
 // Fill c->stats timings from its events (blocks until the commit finished).
-// Events: 0 start, 1 LDEs done, 2 injected-row digests done, 3 leaves done,
-// 4 root ready (all on the compute stream); 5 copies may start, 6 copies
-// done (copy stream).  With host inputs the LDE span includes waiting for
-// the copies it overlaps.
+// Events: 0 start (st), 1 all LDEs done (LDE stream), 2 / 3 around the leaf
+// hashing launch (st), 4 root ready (st), 5 allocations done / copies may
+// start (st), 6 copies done (copy stream).  LDEs and row hashing overlap, so
+// the spans overlap too; with host inputs the LDE span includes waiting for
+// the copies.
 pico_status finish_stats(pico_commit* c) {
   if (!c->ev[4]) return PICO_OK;
   pico_status s;
   if ((s = cuda_status(cudaEventSynchronize(c->ev[4]), "commit events"))) return s;
   if ((s = cuda_status(cudaEventSynchronize(c->ev[6]), "commit events"))) return s;
-  float t[5];
-  for (int i = 0; i < 4; i++)
-    if ((s = cuda_status(cudaEventElapsedTime(&t[i], c->ev[i], c->ev[i + 1]), "event timing"))) return s;
-  if ((s = cuda_status(cudaEventElapsedTime(&t[4], c->ev[5], c->ev[6]), "event timing"))) return s;
-  c->stats.lde_ms = t[0];
-  c->stats.leaves_ms = t[2];
-  c->stats.tree_ms = (double)t[1] + t[3];
-  c->stats.h2d_ms = t[4];
-  c->stats.total_ms = (double)t[0] + t[1] + t[2] + t[3];
+  float t_lde, t_leaf, t_tree, t_tot, t_h2d;
+  if ((s = cuda_status(cudaEventElapsedTime(&t_lde, c->ev[0], c->ev[1]), "event timing"))) return s;
+  if ((s = cuda_status(cudaEventElapsedTime(&t_leaf, c->ev[2], c->ev[3]), "event timing"))) return s;
+  if ((s = cuda_status(cudaEventElapsedTime(&t_tree, c->ev[3], c->ev[4]), "event timing"))) return s;
+  if ((s = cuda_status(cudaEventElapsedTime(&t_tot, c->ev[0], c->ev[4]), "event timing"))) return s;
+  if ((s = cuda_status(cudaEventElapsedTime(&t_h2d, c->ev[5], c->ev[6]), "event timing"))) return s;
+  c->stats.lde_ms = t_lde;
+  c->stats.leaves_ms = t_leaf;
+  c->stats.tree_ms = t_tree;
+  c->stats.h2d_ms = t_h2d;
+  c->stats.total_ms = t_tot;
   for (int e = 0; e < 7; e++) {
     cudaEventDestroy(c->ev[e]);
     c->ev[e] = nullptr;
@@ -635,14 +664,17 @@ static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_mat
     return PICO_ERR_OUT_OF_MEMORY;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t cst;
-  cudaStream_t st = pick_stream(ctx, &cst);
+  cudaStream_t cst, lst;
+  cudaStream_t st = pick_stream(ctx, &cst, &lst);
   auto c = std::make_unique<pico_commit>();
   std::vector<void*> scratch;
   uint32_t root_h[8];
-  s = enqueue_commit(ctx, plan, st, cst, c.get(), scratch, root_h);
-  // On failure the copy stream may still be writing into scratch buffers.
-  if (s) cudaStreamSynchronize(cst);
+  s = enqueue_commit(ctx, plan, st, cst, lst, c.get(), scratch, root_h);
+  // On failure the copy and LDE streams may still be using scratch buffers.
+  if (s) {
+    cudaStreamSynchronize(cst);
+    cudaStreamSynchronize(lst);
+  }
   for (void* p : scratch) cudaFreeAsync(p, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "commit");
   if (!s) s = s2;

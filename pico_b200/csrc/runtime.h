@@ -61,11 +61,11 @@ struct Server;  // serving.h
 
 bool try_reserve(pico_ctx* ctx, uint64_t bytes);
 void unreserve(pico_ctx* ctx, uint64_t bytes);
-cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr);
+cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr, cudaStream_t* lde_stream = nullptr);
 cudaStream_t aux_stream(pico_ctx* ctx);
 TwiddleTables twiddles(pico_ctx* ctx, int field);
 pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
-                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
+                           cudaStream_t lst, pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
 void free_commit_buffers(pico_commit* c, cudaStream_t st);
 pico_status finish_stats(pico_commit* c);
 
@@ -80,6 +80,7 @@ struct pico_ctx {
   std::condition_variable cv;  // signalled whenever reserved memory is returned
   std::vector<cudaStream_t> streams;
   std::vector<cudaStream_t> copy_streams;  // paired with streams[i]: host -> device input copies
+  std::vector<cudaStream_t> lde_streams;   // paired with streams[i]: LDE kernels
   std::atomic<uint32_t> next_stream{0};
   std::vector<cudaStream_t> aux_streams;  // read-backs and releases of finished work
   std::atomic<uint32_t> next_aux{0};

@@ -97,8 +97,12 @@ static void launch_request(Server* sv, pico_request* r) {
   pico_ctx* ctx = sv->ctx;
   cudaStream_t st = ctx->streams[r->slot];
   r->commit = new pico_commit();
-  pico_status s = enqueue_commit(ctx, r->plan, st, ctx->copy_streams[r->slot], r->commit, r->scratch, r->root_pinned);
-  if (s) cudaStreamSynchronize(ctx->copy_streams[r->slot]);  // copies may still target scratch
+  pico_status s = enqueue_commit(ctx, r->plan, st, ctx->copy_streams[r->slot], ctx->lde_streams[r->slot], r->commit,
+                                 r->scratch, r->root_pinned);
+  if (s) {  // copies and LDEs may still target scratch
+    cudaStreamSynchronize(ctx->copy_streams[r->slot]);
+    cudaStreamSynchronize(ctx->lde_streams[r->slot]);
+  }
   for (void* p : r->scratch) cudaFreeAsync(p, st);
   r->scratch.clear();
   if (s == PICO_OK) s = cuda_status(cudaLaunchHostFunc(st, on_request_done, r), "completion callback");
