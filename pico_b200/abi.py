@@ -13,6 +13,8 @@ from pathlib import Path
 from . import build as _build
 
 PICO_OK = 0
+PICO_ERR_INVALID_ARG = 1
+PICO_ERR_UNSUPPORTED = 4
 STATUS_NAMES = {
     0: "PICO_OK",
     1: "PICO_ERR_INVALID_ARG",

@@ -277,6 +277,11 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
       set_error("commit: matrix %u height 2^%u with blowup 2^%u exceeds two-adicity %u", i, m.log_height, log_b, S);
       return PICO_ERR_INVALID_ARG;
     }
+    if (extend && m.log_height > kLdeMaxLogN) {
+      set_error("commit: matrix %u height 2^%u: LDE inputs above 2^%u rows are not supported", i, m.log_height,
+                kLdeMaxLogN);
+      return PICO_ERR_UNSUPPORTED;
+    }
     if (!m.values && m.width) {
       set_error("commit: matrix %u has null values", i);
       return PICO_ERR_INVALID_ARG;
@@ -848,6 +853,10 @@ extern "C" pico_status pico_gpu_coset_lde_batch(pico_ctx* ctx, pico_field field,
   if (log_n + log_blowup > field_two_adicity(field)) {
     set_error("coset_lde_batch: 2^%u rows with blowup 2^%u exceeds the two-adicity", log_n, log_blowup);
     return PICO_ERR_INVALID_ARG;
+  }
+  if (log_n > kLdeMaxLogN) {
+    set_error("coset_lde_batch: inputs above 2^%u rows are not supported", kLdeMaxLogN);
+    return PICO_ERR_UNSUPPORTED;
   }
   if (flags & PICO_LDE_NATURAL_ORDER) {
     set_error("coset_lde_batch: natural row order is not implemented; the committed order is bit-reversed");

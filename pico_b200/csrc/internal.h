@@ -76,6 +76,7 @@ struct LdeMat {
   uint32_t shift;          // coset shift, Monty form
 };
 constexpr int kLdeSmallMaxLog = 11;  // one-pass form handles n <= 2^11
+constexpr uint32_t kLdeMaxLogN = 24;  // coset power tables cover exponents below 2^24
 constexpr int kLdeBatch = 32;        // matrices per launch (descriptors travel as kernel parameters)
 struct LdeBatch {
   uint32_t n;

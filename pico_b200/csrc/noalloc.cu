@@ -100,6 +100,10 @@ extern "C" pico_status pico_gpu_coset_lde_batch_noalloc(pico_field field, const 
               S);
     return PICO_ERR_INVALID_ARG;
   }
+  if (log_n > kLdeMaxLogN) {
+    set_error("coset_lde_batch_noalloc: inputs above 2^%u rows are not supported", kLdeMaxLogN);
+    return PICO_ERR_UNSUPPORTED;
+  }
   const uint64_t n = 1ull << log_n;
   const uint64_t pw_words = (uint64_t)kPwWords << log_blowup;
   const bool three_pass = (int)log_n > kLdeSmallMaxLog;

@@ -208,6 +208,12 @@ def test_invalid_shapes_are_reported(gpu):
     # 2^23 rows with blowup 4 exceeds KoalaBear's two-adicity 24
     with pytest.raises(PicoError):
         abi.check(gpu.lib.pico_gpu_commit(gpu.handle, 0, mats, 1, 2, 0, None, root))
+    # BabyBear admits 2^25 x 2, but LDE inputs above 2^24 rows are refused
+    # before any buffer is touched
+    mats[0].log_height = 25
+    with pytest.raises(PicoError) as e:
+        abi.check(gpu.lib.pico_gpu_commit(gpu.handle, 1, mats, 1, 1, 0, None, root))
+    assert e.value.status == abi.PICO_ERR_UNSUPPORTED
 
 
 # ---------------------------------------------------------------- FRI
