@@ -71,6 +71,8 @@ WORKLOADS = {
     # same shape distribution scaled to 2^25 cells (heights 2^6..2^18): for profiler captures
     "uneven-kb-2^25": dict(field=0, log_blowup=1, shapes=lambda: uneven_kb_shapes(target_log=25, lo=6, hi=18),
                            seed=2),
+    # one tall narrow trace (2^11-point sub-transforms, ~2 GB on the device): for profiler captures
+    "single-kb-2^22x16": dict(field=0, log_blowup=1, shapes=lambda: [(22, 16)], seed=4),
 }
 
 
@@ -135,9 +137,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
-PERM_MONTMULS = {0: 8 * 16 * 2 + 20 * 2, 1: 8 * 16 * 4 + 13 * 4}  # S-box Montgomery products per permutation
-IMAD_PER_MONTMUL = 3  # a*b wide, q = lo * (-1/p), q*p + t wide
+# Algorithmic Poseidon2 work: modular multiplications per permutation (S-box
+# products plus one internal-diagonal product per lane per partial round;
+# additions excluded): KoalaBear 8*16*2 + 20*2 + 20*16, BabyBear
+# 8*16*4 + 13*4 + 13*16.  One Montgomery product ~ 4 IMAD-pipe instructions.
+PERM_MODMULS = {0: 8 * 16 * 2 + 20 * 2 + 20 * 16, 1: 8 * 16 * 4 + 13 * 4 + 13 * 16}
+IMAD_PER_MODMUL = 4
 IMAD_PER_SM_CLK = 64
+# DRAM bytes per algorithmic byte of one leaf-hashing launch (dram__bytes_read
+# + dram__bytes_write over rows * (4 * width + 32)), from an ncu capture of
+# k_hash_rows on a 2^23-row x 16-column LDE (the single-kb-2^22x16 workload)
+HASH_TRAFFIC_RATIO = 0.966
 
 
 def dist_setup(n_gpus: int):
@@ -277,6 +287,33 @@ def run_gpu(args, rank, world, local):
     # plain per-matrix form (the baseline form), same inputs
     ms_plain, _, _ = timed(traces, plain=True) if not args.skip_plain else (None, None, None)
 
+    # LDE kernels alone (no hashing sharing the SMs): every matrix of the
+    # workload through coset_lde_batch, device in and out
+    lde_only_ms = None
+    if not args.skip_lde:
+        from pico_b200 import Radix2DitParallel
+
+        dft = Radix2DitParallel(ctx, field)
+        shift = F.lde_shift(field)
+        outs = [torch.empty((1 << (lh + b), w), dtype=torch.int32, device=dev) for lh, w in shapes]
+
+        def lde_all():
+            for t, o in zip(traces, outs):
+                if t.numel():
+                    dft.coset_lde_batch_bitrev(t, b, shift, out=o)
+
+        lde_all()
+        torch.cuda.synchronize()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record()
+        for _ in range(args.steps):
+            lde_all()
+        l1.record()
+        l1.synchronize()
+        lde_only_ms = l0.elapsed_time(l1) / args.steps
+        del outs
+        torch.cuda.empty_cache()
+
     # e2e: pinned host inputs through the C ABI, copies inside the timed region
     e2e = None
     if not args.skip_e2e:
@@ -296,13 +333,16 @@ def run_gpu(args, rank, world, local):
     # roofline of the dominant kernel: Poseidon2 leaf hashing (integer-multiply bound)
     s0 = stats[-1]
     leaves_s = float(np.mean([s["leaves_ms"] for s in stats])) / 1e3
-    lde_s = float(np.mean([s["lde_ms"] for s in stats])) / 1e3
     mhz = clocks["sm_mhz"] or 1965.0
     sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
     imad_peak = sm_count * IMAD_PER_SM_CLK * mhz * 1e6 / 1e12  # Tops/s
-    imad_ach = s0["leaf_permutations"] * PERM_MONTMULS[field] * IMAD_PER_MONTMUL / leaves_s / 1e12
+    imad_ach = s0["leaf_permutations"] * PERM_MODMULS[field] * IMAD_PER_MODMUL / leaves_s / 1e12
+    leaf_rows = 1 << max(lh for lh, _ in shapes) + b
+    leaf_width = sum(w for lh, w in shapes if lh == max(l for l, _ in shapes))
+    leaf_bytes = leaf_rows * (4 * leaf_width + 32)
     hbm_peak, hbm_kind = peaks()
-    lde_ach = s0["lde_bytes"] / lde_s / 1e9
+    lde_alg_bytes = 4 * sum(w * ((1 << lh) + (1 << (lh + b))) for lh, w in shapes)
+    lde_ach = lde_alg_bytes / (lde_only_ms / 1e3) / 1e9 if lde_only_ms else None
     result = {
         "metric": METRIC,
         "value": value,
@@ -324,29 +364,35 @@ def run_gpu(args, rank, world, local):
             "field": F.NAMES[field],
             "form": "batched",
             "parallelism": f"replicas x{world}",
-            "l2": "inputs (4 GiB) larger than L2; no flush",
+            "l2": f"inputs ({in_bytes / 2**30:.2f} GiB) larger than L2 (126 MB); no flush"
+                  if in_bytes > 126e6 else "inputs smaller than L2: not flushed",
         },
         "gpu_launches": int(sum(s["launches"] for s in stats)),
         "clocks": clocks,
         "roofline": {
-            "kernel": "k_hash_rows (Poseidon2 leaf hashing)",
+            "kernel": "k_hash_rows (Poseidon2 leaf hashing, one launch per commit)",
             "bound": "imad",
             "achieved": imad_ach,
             "peak": imad_peak,
             "unit": "Tops/s",
             "frac": imad_ach / imad_peak,
-            "traffic": None,
-            "note": f"algorithmic IMAD-pipe ops = S-box Montgomery products ({PERM_MONTMULS[field]}/perm) x 3; "
-                    f"peak = {sm_count} SMs x {IMAD_PER_SM_CLK}/clk x median SM clock",
+            "traffic": leaf_bytes * HASH_TRAFFIC_RATIO,
+            "algorithmic_bytes": leaf_bytes,
+            "launch_ms": leaves_s * 1e3,
+            "note": f"integer-multiply bound: achieved = {IMAD_PER_MODMUL} IMAD x {PERM_MODMULS[field]} modmuls "
+                    f"x leaf permutations / launch time; peak = {sm_count} SMs x {IMAD_PER_SM_CLK} IMAD/clk x "
+                    f"median SM clock; traffic = algorithmic bytes x the DRAM/algorithmic ratio ncu measured",
         },
         "roofline_lde": {
-            "kernel": "LDE kernels (k_lde_*)",
+            "kernel": "LDE kernels (k_pow_tables + k_lde_*), timed alone through coset_lde_batch",
             "bound": "hbm",
             "achieved": lde_ach,
             "peak": hbm_peak,
             "unit": "GB/s",
-            "frac": lde_ach / hbm_peak,
+            "frac": lde_ach / hbm_peak if lde_ach else None,
             "traffic": None,
+            "algorithmic_bytes": lde_alg_bytes,
+            "ms": lde_only_ms,
             "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback",
         },
         "phases_ms": {k: float(np.mean([s[k] for s in stats])) for k in ("lde_ms", "leaves_ms", "tree_ms", "total_ms")},
@@ -540,6 +586,7 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-lde", action="store_true", help="skip the LDE-alone timing")
     args = ap.parse_args()
 
     rank, world, local = dist_setup(args.gpus)

@@ -148,8 +148,6 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
     ctx->streams.push_back(st);
     if ((s = cuda_status(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
     ctx->copy_streams.push_back(cst);
-    if ((s = cuda_status(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
-    ctx->lde_streams.push_back(cst);
   }
   for (uint32_t i = 0; i < 4; i++) {
     cudaStream_t st;
@@ -171,10 +169,23 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
     else
       host_twiddles<BabyBear>(t);
     void* d = nullptr;
-    if ((s = cuda_status(cudaMalloc(&d, t.size() * 4), "twiddle tables"))) return s;
+    if ((s = cuda_status(cudaMalloc(&d, (2 * kTwiddleWords + kStageTableWords) * 4), "twiddle tables"))) return s;
+    ctx->tw[f] = (uint32_t*)d;
     if ((s = cuda_status(cudaMemcpy(d, t.data(), t.size() * 4, cudaMemcpyHostToDevice), "twiddle upload")))
       return s;
-    ctx->tw[f] = (uint32_t*)d;
+    const TwiddleTables tt = twiddles(ctx.get(), f);
+    if ((s = cuda_status(launch_stage_tables(f, tt, const_cast<uint32_t*>(tt.stage), nullptr), "stage tables")) ||
+        (s = cuda_status(cudaDeviceSynchronize(), "stage tables")))
+      return s;
+  }
+  {
+    void* g = nullptr;
+    const size_t bytes = 2 * ctx->streams.size() * sizeof(GuardRecord);
+    if ((s = cuda_status(cudaMallocHost(&g, bytes), "guard records"))) return s;
+    memset(g, 0, bytes);
+    ctx->guard_host = (GuardRecord*)g;
+    if ((s = cuda_status(lde_guard_clear(), "guard clear")) || (s = cuda_status(hash_guard_clear(), "guard clear")))
+      return s;
   }
   if ((s = serving_start(ctx.get()))) return s;
   *out = ctx.release();
@@ -193,16 +204,13 @@ extern "C" pico_status pico_gpu_shutdown(pico_ctx* ctx) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
-  for (auto st : ctx->lde_streams) {
-    cudaStreamSynchronize(st);
-    cudaStreamDestroy(st);
-  }
   for (auto st : ctx->aux_streams) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
   for (int f = 0; f < 2; f++)
     if (ctx->tw[f]) cudaFree(ctx->tw[f]);
+  if (ctx->guard_host) cudaFreeHost(ctx->guard_host);
   delete ctx;
   return PICO_OK;
 }
@@ -238,16 +246,43 @@ cudaStream_t aux_stream(pico_ctx* ctx) {
   return ctx->aux_streams[i];
 }
 
-cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream, cudaStream_t* lde_stream) {
+cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream, uint32_t* slot) {
   uint32_t i = ctx->next_stream.fetch_add(1) % (uint32_t)ctx->streams.size();
   if (copy_stream) *copy_stream = ctx->copy_streams[i];
-  if (lde_stream) *lde_stream = ctx->lde_streams[i];
+  if (slot) *slot = i;
   return ctx->streams[i];
+}
+
+pico_status guard_enqueue(pico_ctx* ctx, uint32_t slot, cudaStream_t st) {
+  pico_status s;
+  if ((s = cuda_status(lde_guard_fetch(ctx->guard_host + 2 * slot, st), "guard read-back"))) return s;
+  return cuda_status(hash_guard_fetch(ctx->guard_host + 2 * slot + 1, st), "guard read-back");
+}
+
+pico_status guard_verdict(pico_ctx* ctx, uint32_t slot, std::string* msg) {
+  static const char* const unit[2] = {"LDE", "row hashing"};
+  for (int u = 0; u < 2; u++) {
+    const GuardRecord& g = ctx->guard_host[2 * slot + u];
+    if (!g.count) continue;
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "internal bounds guard: %s kernel skipped %llu access(es); first: tag %llu, offset %llu of %llu, "
+             "block %llu, thread %llu",
+             unit[u], g.count, g.tag, g.offset, g.extent, g.block, g.thread);
+    if (msg) *msg = buf;
+    set_error("%s", buf);
+    lde_guard_clear();
+    hash_guard_clear();
+    memset(ctx->guard_host + 2 * slot, 0, 2 * sizeof(GuardRecord));
+    return PICO_ERR_CUDA;
+  }
+  return PICO_OK;
 }
 TwiddleTables twiddles(pico_ctx* ctx, int field) {
   TwiddleTables t;
   t.lo = ctx->tw[field];
-  t.hi = ctx->tw[field] + 16384;
+  t.hi = ctx->tw[field] + kTwiddleWords;
+  t.stage = ctx->tw[field] + 2 * kTwiddleWords;
   return t;
 }
 
@@ -346,9 +381,9 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   return PICO_OK;
 }
 
-// Enqueue a whole commit: Poseidon2 on `st`, LDEs on `lst`, host -> device
-// input copies on `cst` (three streams, so copies, LDEs and hashing overlap).  On success `c` holds
-// the resident buffers and `scratch` the buffers to free once `st` has passed
+// Enqueue a whole commit: LDEs and Poseidon2 on `st`, host -> device input
+// copies on `cst`, so copies overlap the compute.  On success `c` holds the
+// resident buffers and `scratch` the buffers to free once `st` has passed
 // this point (the caller frees them on `st`, which waits for `cst`).
 //
 // Order of work.  The tree needs every height group's rows: the tallest
@@ -357,7 +392,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
 // of the short groups run while the tallest group is still in transit; the
 // tallest group's LDE, its leaf hashing and the compression levels come last.
 pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
-                           cudaStream_t lst, pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
+                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
   pico_status s;
   const int field = plan.field;
   const uint32_t n = (uint32_t)plan.mats.size();
@@ -387,7 +422,9 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   for (uint32_t k = 0; k < n; k++) {
     const PlannedMat& m = plan.mats[k];
     in_bytes[k] = ((uint64_t)m.w << m.log_n) * 4;
-    if (!copy_in || in_bytes[k] == 0) {
+    if (in_bytes[k] == 0) {
+      dev_in[k] = nullptr;  // a width-0 matrix: nothing to read, on either side
+    } else if (!copy_in) {
       dev_in[k] = m.src;
     } else {
       void* d;
@@ -503,89 +540,65 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     if ((s = cuda_status(cudaEventRecord(c->ev[6], st), "event"))) return s;
   }
 
-  // ---- compute: LDEs on lst, Poseidon2 on st, pipelined per height group ----
-  // The LDE of one group runs while the previous group's rows are hashed:
-  // the LDE kernels stall on memory latency while hashing saturates the
-  // integer pipes, so the two share the SMs well.
+  // ---- compute on st, one height group at a time ----
+  // Shortest group first (the order host copies arrive in): its LDE, then
+  // the digests of its rows; the tallest group's rows are the leaves and come
+  // last, then the compression levels.  Each phase of each group sits
+  // between a pair of events, so the timings add up exactly.
   const TwiddleTables tw = twiddles(ctx, field);
+  // Width-0 matrices add nothing to a row, so they get no segment.
   auto make_group = [&](uint32_t gi, RowGroup& g) {
     memset(&g, 0, sizeof g);
     const auto& gr = plan.groups[gi];
-    g.n_segs = gr.second - gr.first;
     for (uint32_t k = gr.first; k < gr.second; k++) {
-      g.segs[k - gr.first].ptr = leaves[k];
-      g.segs[k - gr.first].width = plan.mats[k].w;
+      if (plan.mats[k].w == 0) continue;
+      g.segs[g.n_segs].ptr = leaves[k];
+      g.segs[g.n_segs].width = plan.mats[k].w;
+      g.n_segs++;
       g.total_width += plan.mats[k].w;
     }
   };
+  // Width-0 matrices have no LDE work and are left out of the launches.
   auto lde_group = [&](uint32_t first, uint32_t last) -> pico_status {
-    if (!plan.extend || first == last) return PICO_OK;
+    if (!plan.extend) return PICO_OK;
+    std::vector<LdeMat> mats;
+    for (uint32_t k = first; k < last; k++)
+      if (hm[k].w) mats.push_back(hm[k]);
+    if (mats.empty()) return PICO_OK;
     if (plan.plain) {
-      for (uint32_t k = first; k < last; k++)
-        if (pico_status r = cuda_status(launch_lde(field, &hm[k], 1, tw, lst, &c->stats.launches), "LDE launch"))
+      for (const LdeMat& m : mats)
+        if (pico_status r = cuda_status(launch_lde(field, &m, 1, tw, st, &c->stats.launches), "LDE launch"))
           return r;
       return PICO_OK;
     }
-    return cuda_status(launch_lde(field, &hm[first], last - first, tw, lst, &c->stats.launches), "LDE launch");
+    return cuda_status(launch_lde(field, mats.data(), (uint32_t)mats.size(), tw, st, &c->stats.launches),
+                       "LDE launch");
   };
-  // Device inputs: tallest group first (its leaf hashing is the longest job).
-  // Host inputs: the order the copies arrive in (shortest first).
-  std::vector<uint32_t> order;
-  for (uint32_t i = 0; i < G; i++) order.push_back(copy_in ? G - 1 - i : i);
-  std::vector<cudaEvent_t> lde_done(G, nullptr);
-  auto destroy_all = [&]() {
-    destroy_events();
-    for (auto e : lde_done)
-      if (e) cudaEventDestroy(e);
-  };
-  if ((s = cuda_status(cudaStreamWaitEvent(lst, c->ev[5], 0), "LDE stream wait"))) {
-    destroy_all();
-    return s;
-  }
-  for (uint32_t gi : order) {
-    if (copy_in && (s = cuda_status(cudaStreamWaitEvent(lst, arrived[gi], 0), "wait for inputs"))) {
-      destroy_all();
+  c->group_ev.assign(4 * G, nullptr);
+  for (auto& e : c->group_ev)
+    if ((s = cuda_status(cudaEventCreate(&e), "event"))) {
+      destroy_events();
       return s;
     }
-    if ((s = lde_group(plan.groups[gi].first, plan.groups[gi].second))) {
-      destroy_all();
-      return s;
-    }
-    if ((s = cuda_status(cudaEventCreateWithFlags(&lde_done[gi], cudaEventDisableTiming), "event")) ||
-        (s = cuda_status(cudaEventRecord(lde_done[gi], lst), "event"))) {
-      destroy_all();
-      return s;
-    }
-  }
-  if ((s = cuda_status(cudaEventRecord(c->ev[1], lst), "event"))) {
-    destroy_all();
-    return s;
-  }
   uint32_t* layer = c->layers;
-  for (uint32_t gi : order) {
-    if ((s = cuda_status(cudaStreamWaitEvent(st, lde_done[gi], 0), "wait for LDE"))) {
-      destroy_all();
-      return s;
-    }
+  for (uint32_t gi = G; gi-- > 0;) {
+    cudaEvent_t* ge = &c->group_ev[4 * gi];
+    if (copy_in && (s = cuda_status(cudaStreamWaitEvent(st, arrived[gi], 0), "wait for inputs"))) break;
+    if ((s = cuda_status(cudaEventRecord(ge[0], st), "event"))) break;
+    if ((s = lde_group(plan.groups[gi].first, plan.groups[gi].second))) break;
+    if ((s = cuda_status(cudaEventRecord(ge[1], st), "event"))) break;
     RowGroup g;
     make_group(gi, g);
-    if (gi == 0 && (s = cuda_status(cudaEventRecord(c->ev[2], st), "event"))) {
-      destroy_all();
-      return s;
-    }
+    if ((s = cuda_status(cudaEventRecord(ge[2], st), "event"))) break;
     s = cuda_status(launch_hash_rows(field, g, 1ull << plan.mats[plan.groups[gi].first].log_N,
                                      gi == 0 ? layer : inj[gi], st),
                     gi == 0 ? "leaf hashing" : "row hashing");
     c->stats.launches += 1;
-    if (!s && gi == 0) s = cuda_status(cudaEventRecord(c->ev[3], st), "event");
-    if (s) {
-      destroy_all();
-      return s;
-    }
+    if (s || (s = cuda_status(cudaEventRecord(ge[3], st), "event"))) break;
   }
-  destroy_all();
-  // the tree below needs every LDE; the last lde_done wait covered all of them
-  // (the LDE stream runs the groups in order)
+  destroy_events();
+  if (s) return s;
+  if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;
   uint32_t next_group = 1;
   for (uint32_t lvl = 1; lvl <= log_max; lvl++) {
     const uint64_t len = 1ull << (log_max - lvl);
@@ -603,31 +616,37 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
 }
 
 // Fill c->stats timings from its events (blocks until the commit finished).
-// Events: 0 start (st), 1 all LDEs done (LDE stream), 2 / 3 around the leaf
-// hashing launch (st), 4 root ready (st), 5 allocations done / copies may
-// start (st), 6 copies done (copy stream).  LDEs and row hashing overlap, so
-// the spans overlap too; with host inputs the LDE span includes waiting for
-// the copies.
+// Events: 0 start (st), 3 compression starts (st), 4 root ready (st), 5
+// allocations done / copies may start (st), 6 copies done (copy stream);
+// per height group g, group_ev[4g .. 4g+3] bracket its LDE and its row
+// hashing on st.  lde_ms sums the LDE brackets, leaves_ms is the tallest
+// group's hashing, tree_ms the other groups' row digests plus compression.
 pico_status finish_stats(pico_commit* c) {
   if (!c->ev[4]) return PICO_OK;
   pico_status s;
   if ((s = cuda_status(cudaEventSynchronize(c->ev[4]), "commit events"))) return s;
   if ((s = cuda_status(cudaEventSynchronize(c->ev[6]), "commit events"))) return s;
-  float t_lde, t_leaf, t_tree, t_tot, t_h2d;
-  if ((s = cuda_status(cudaEventElapsedTime(&t_lde, c->ev[0], c->ev[1]), "event timing"))) return s;
-  if ((s = cuda_status(cudaEventElapsedTime(&t_leaf, c->ev[2], c->ev[3]), "event timing"))) return s;
-  if ((s = cuda_status(cudaEventElapsedTime(&t_tree, c->ev[3], c->ev[4]), "event timing"))) return s;
-  if ((s = cuda_status(cudaEventElapsedTime(&t_tot, c->ev[0], c->ev[4]), "event timing"))) return s;
-  if ((s = cuda_status(cudaEventElapsedTime(&t_h2d, c->ev[5], c->ev[6]), "event timing"))) return s;
+  auto span = [&](cudaEvent_t a, cudaEvent_t b, double& acc) -> pico_status {
+    float t = 0;
+    pico_status r = cuda_status(cudaEventElapsedTime(&t, a, b), "event timing");
+    acc += t;
+    return r;
+  };
+  double t_lde = 0, t_leaf = 0, t_tree = 0, t_tot = 0, t_h2d = 0;
+  const size_t G = c->group_ev.size() / 4;
+  for (size_t g = 0; g < G; g++) {
+    if ((s = span(c->group_ev[4 * g], c->group_ev[4 * g + 1], t_lde))) return s;
+    if ((s = span(c->group_ev[4 * g + 2], c->group_ev[4 * g + 3], g == 0 ? t_leaf : t_tree))) return s;
+  }
+  if ((s = span(c->ev[3], c->ev[4], t_tree))) return s;
+  if ((s = span(c->ev[0], c->ev[4], t_tot))) return s;
+  if ((s = span(c->ev[5], c->ev[6], t_h2d))) return s;
   c->stats.lde_ms = t_lde;
   c->stats.leaves_ms = t_leaf;
   c->stats.tree_ms = t_tree;
   c->stats.h2d_ms = t_h2d;
   c->stats.total_ms = t_tot;
-  for (int e = 0; e < 7; e++) {
-    cudaEventDestroy(c->ev[e]);
-    c->ev[e] = nullptr;
-  }
+  c->destroy_events();
   return PICO_OK;
 }
 
@@ -641,10 +660,16 @@ void free_commit_buffers(pico_commit* c, cudaStream_t st) {
 
 }  // namespace pico
 
-pico_commit::~pico_commit() {
+void pico_commit::destroy_events() {
   for (int e = 0; e < 7; e++)
     if (ev[e]) cudaEventDestroy(ev[e]);
+  for (cudaEvent_t e : group_ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t& e : ev) e = nullptr;
+  group_ev.clear();
 }
+
+pico_commit::~pico_commit() { destroy_events(); }
 
 static thread_local pico_commit_stats g_last_stats{};
 
@@ -669,20 +694,20 @@ static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_mat
     return PICO_ERR_OUT_OF_MEMORY;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t cst, lst;
-  cudaStream_t st = pick_stream(ctx, &cst, &lst);
+  cudaStream_t cst;
+  uint32_t slot = 0;
+  cudaStream_t st = pick_stream(ctx, &cst, &slot);
   auto c = std::make_unique<pico_commit>();
   std::vector<void*> scratch;
   uint32_t root_h[8];
-  s = enqueue_commit(ctx, plan, st, cst, lst, c.get(), scratch, root_h);
-  // On failure the copy and LDE streams may still be using scratch buffers.
-  if (s) {
-    cudaStreamSynchronize(cst);
-    cudaStreamSynchronize(lst);
-  }
+  s = enqueue_commit(ctx, plan, st, cst, c.get(), scratch, root_h);
+  // On failure the copy stream may still be writing scratch buffers.
+  if (s) cudaStreamSynchronize(cst);
   for (void* p : scratch) cudaFreeAsync(p, st);
+  if (!s) s = guard_enqueue(ctx, slot, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "commit");
   if (!s) s = s2;
+  if (!s) s = guard_verdict(ctx, slot);
   unreserve(ctx, plan.bytes_scratch);
   if (s) {
     free_commit_buffers(c.get(), st);
@@ -873,7 +898,8 @@ extern "C" pico_status pico_gpu_coset_lde_batch(pico_ctx* ctx, pico_field field,
     return PICO_ERR_OUT_OF_MEMORY;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  uint32_t slot = 0;
+  cudaStream_t st = pick_stream(ctx, nullptr, &slot);
   std::vector<void*> scratch;
   // Reuse the commit planner's LDE path without the tree: build the LdeMat directly.
   LdeMat L;
@@ -921,9 +947,12 @@ extern "C" pico_status pico_gpu_coset_lde_batch(pico_ctx* ctx, pico_field field,
   };
   s = run();
   for (void* p : scratch) cudaFreeAsync(p, st);
+  if (!s) s = guard_enqueue(ctx, slot, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "coset_lde_batch");
+  if (!s) s = s2;
+  if (!s) s = guard_verdict(ctx, slot);
   unreserve(ctx, need);
-  return s ? s : s2;
+  return s;
 }
 
 extern "C" pico_status pico_gpu_poseidon2_permute(pico_ctx* ctx, pico_field field, uint32_t* states, uint64_t n,

@@ -51,7 +51,8 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
     return PICO_ERR_OUT_OF_MEMORY;
   }
   cudaSetDevice(ctx->device);
-  cudaStream_t st = pick_stream(ctx);
+  uint32_t slot = 0;
+  cudaStream_t st = pick_stream(ctx, nullptr, &slot);
   auto f = std::make_unique<pico_fri>();
   f->ctx = ctx;
   f->field = field;
@@ -171,8 +172,10 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
   };
   pico_status s = run();
   for (void* p : scratch) cudaFreeAsync(p, st);
+  if (!s) s = guard_enqueue(ctx, slot, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "fri_commit_phase");
   if (!s) s = s2;
+  if (!s) s = guard_verdict(ctx, slot);
   unreserve(ctx, small);
   if (!s && log_final_len == 0) {
     // Plonky3 asserts the remaining 2^b evaluations of the constant polynomial agree.

@@ -44,11 +44,37 @@ struct DevChallenger {
   uint32_t out_buf[8];
   uint32_t out_len;
 };
-// Per-field twiddle tables: lo[j] = w^j, hi[j] = w^(j * 2^14), w of order 2^S.
+// First out-of-range access a guarded kernel skipped (count = accesses
+// skipped since the last clear).  Tags name the kind of access.
+struct GuardRecord {
+  unsigned long long count, tag, offset, extent, block, thread, pad[2];
+};
+enum GuardTag : int {
+  kGuardLoad = 1,       // LDE global load (offset / extent in words of the pass's input)
+  kGuardStore = 2,      // LDE global store (offset / extent in words of the pass's output)
+  kGuardRowRead = 10,   // row hashing: segment index / column
+  kGuardTile = 100,     // LDE shared-memory tile index
+  kGuardTwiddle = 101,  // LDE shared-memory twiddle index
+  kGuardPowIndex = 102  // coset power-table exponent
+};
+// Asynchronous copy of a unit's record to host memory on st / synchronous clear.
+cudaError_t lde_guard_fetch(GuardRecord* dst, cudaStream_t st);
+cudaError_t lde_guard_clear();
+cudaError_t hash_guard_fetch(GuardRecord* dst, cudaStream_t st);
+cudaError_t hash_guard_clear();
+
+// Per-field twiddle tables: lo[j] = w^j, hi[j] = w^(j * 2^14), w of order 2^S;
+// `stage`: the per-stage tables of every sub-transform length 2^l, l = 1..12,
+// in the layout the LDE kernels copy into shared memory (launch_stage_tables).
 struct TwiddleTables {
   const uint32_t* lo;
   const uint32_t* hi;
+  const uint32_t* stage;
 };
+constexpr uint32_t kTwiddleWords = 16384;     // words of lo, and of hi
+constexpr uint32_t kStageTableWords = 16384;  // words of stage (16380 used)
+// Fill `stage` (kStageTableWords words) from lo/hi of the same field.
+cudaError_t launch_stage_tables(int field, TwiddleTables tw, uint32_t* stage, cudaStream_t st);
 // Fold one codeword of 2^log_len EF4 elements to half length with the EF4
 // challenge at beta (device, 4 words).
 cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,

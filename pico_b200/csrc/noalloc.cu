@@ -12,7 +12,7 @@
 //
 // Costs and rules of the static arrays:
 //   - every GPU that loads this library holds kNoAllocScratchWords * 4 bytes
-//     (32 MiB) plus 256 KiB of twiddles until the process exits;
+//     (32 MiB) plus 384 KiB of twiddles until the process exits;
 //   - all calls share the one scratch array: calls that overlap on the GPU
 //     (two streams, or two host threads) race on it and corrupt each other's
 //     results; serialise them on one stream;
@@ -39,8 +39,9 @@ constexpr uint64_t kNoAllocScratchWords = 8ull << 20;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocScratchWords];
-// Per field: lo[j] = w^j, hi[j] = w^(j * 2^14), w of order 2^two_adicity.
-static __device__ __align__(256) uint32_t g_noalloc_twiddles[2][2 * 16384];
+// Per field: lo[j] = w^j, hi[j] = w^(j * 2^14), w of order 2^two_adicity,
+// then the LDE kernels' per-stage tables.
+static __device__ __align__(256) uint32_t g_noalloc_twiddles[2][2 * pico::kTwiddleWords + pico::kStageTableWords];
 
 template <class F>
 __global__ void k_fill_twiddles(uint32_t* t) {
@@ -72,10 +73,19 @@ pico_status setup_current_device(int dev, cudaStream_t st, DeviceState& out) {
     rc = pico::cuda_status(cudaGetSymbolAddress(&p, g_noalloc_twiddles), "twiddle symbol address");
     if (rc) return rc;
     s.twiddles = (uint32_t*)p;
+    constexpr uint32_t per_field = 2 * pico::kTwiddleWords + pico::kStageTableWords;
     k_fill_twiddles<pico::KoalaBear><<<128, 256, 0, st>>>(s.twiddles);
-    k_fill_twiddles<pico::BabyBear><<<128, 256, 0, st>>>(s.twiddles + 2 * 16384);
+    k_fill_twiddles<pico::BabyBear><<<128, 256, 0, st>>>(s.twiddles + per_field);
     rc = pico::cuda_status(cudaGetLastError(), "twiddle fill");
     if (rc) return rc;
+    for (int f = 0; f < 2; f++) {
+      pico::TwiddleTables tt;
+      tt.lo = s.twiddles + f * per_field;
+      tt.hi = tt.lo + pico::kTwiddleWords;
+      tt.stage = tt.lo + 2 * pico::kTwiddleWords;
+      rc = pico::cuda_status(pico::launch_stage_tables(f, tt, const_cast<uint32_t*>(tt.stage), st), "stage tables");
+      if (rc) return rc;
+    }
     rc = pico::cuda_status(cudaStreamSynchronize(st), "twiddle fill");
     if (rc) return rc;
     s.ready = true;
@@ -141,7 +151,8 @@ extern "C" pico_status pico_gpu_coset_lde_batch_noalloc(pico_field field, const 
     L.t2 = L.t1 + (uint64_t)width * n;
   }
   TwiddleTables tw;
-  tw.lo = ds.twiddles + (uint64_t)field * 2 * 16384;
-  tw.hi = tw.lo + 16384;
+  tw.lo = ds.twiddles + (uint64_t)field * (2 * kTwiddleWords + kStageTableWords);
+  tw.hi = tw.lo + kTwiddleWords;
+  tw.stage = tw.lo + 2 * kTwiddleWords;
   return cuda_status(launch_lde(field, &L, 1, tw, st), "coset_lde_batch_noalloc launch");
 }

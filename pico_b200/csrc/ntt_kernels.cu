@@ -43,6 +43,35 @@
 
 namespace pico {
 
+// Bounds guards.  Every global load and store of these kernels is checked
+// against the buffer it belongs to (the pass's input and output, set per CTA
+// in s_in / s_out), and every shared-memory and twiddle index against its
+// table; an access outside is skipped and the first one is recorded in
+// g_lde_guard, which the entry points copy back with their final
+// synchronisation and report as an error.  The checks cost no measurable
+// time (these kernels wait on memory and barriers, not on issue slots).
+__device__ GuardRecord g_lde_guard;
+struct GuardRange {
+  const uint32_t* lo;
+  const uint32_t* hi;
+};
+__shared__ GuardRange s_in, s_out;
+__shared__ uint32_t s_smem_words;
+__device__ __noinline__ void guard_trip(int tag, unsigned long long offset, unsigned long long extent) {
+  if (atomicAdd(&g_lde_guard.count, 1ull) == 0) {
+    g_lde_guard.tag = tag;
+    g_lde_guard.offset = offset;
+    g_lde_guard.extent = extent;
+    g_lde_guard.block = blockIdx.x;
+    g_lde_guard.thread = threadIdx.x;
+  }
+}
+__device__ __forceinline__ bool in_range(const uint32_t* p, const GuardRange& r, int tag) {
+  if (p >= r.lo && p < r.hi) return true;
+  guard_trip(tag, (unsigned long long)(p - r.lo), (unsigned long long)(r.hi - r.lo));
+  return false;
+}
+
 constexpr int kLogTile = 13;   // words per tile for l >= 4: 2^13 (32 KiB)
 constexpr int kThreads = 512;  // one 16-element set per thread in a four-stage round
 constexpr int kMinLogL3 = 6;   // smallest sub-transform of the three-pass form (n = 2^12)
@@ -129,6 +158,7 @@ __device__ __forceinline__ uint32_t omega(const TwiddleTables& tw, uint32_t log_
 __device__ __forceinline__ const uint32_t* pw_table(const LdeMat& M, uint32_t cb) { return M.pw + cb * kPwWords; }
 template <class F>
 __device__ __forceinline__ uint32_t pw_at(const uint32_t* t, uint32_t i) {
+  if (i >= (1u << 24)) { guard_trip(kGuardPowIndex, i, 1u << 24); i = 0; }
   return Fp<F>::mul(__ldg(t + 4096 + (i >> 12)), __ldg(t + (i & 4095u)));
 }
 
@@ -150,10 +180,61 @@ __device__ __forceinline__ const LdeMat& find_tile(const LdeBatch& B, int pass, 
   return B.m[k];
 }
 
-template <class F, int LOG_L>
-__device__ __forceinline__ void fill_twiddles(uint32_t* t, bool inv, const TwiddleTables& tw) {
-  constexpr uint32_t h = (1u << LOG_L) >> 1;
-  for (uint32_t i = threadIdx.x; i < h; i += kThreads) t[i] = omega<F>(tw, LOG_L, i, inv);
+// Twiddles of a 2^LOG_L-point transform in shared memory, one table per
+// stage: stage s holds w_L^(+-(x << s)) for x < L >> (s+1) at offset
+// L - (L >> s) (L - 1 words in all).  A round's threads read consecutive x,
+// which sit on distinct banks.  The exception is the fused first forward
+// round, whose x differ in bits 4 .. l-5 (x = rev(q) + c * L/16); for
+// l >= 9 (fewer than 32 lines) the tables of stages 0..3 therefore store
+// entry x at x ^ ((x >> 4) & (2^(l-8) - 1)).  Every access to those tables
+// has x = o + c * L/16 with o < L/16, so the swizzle applies to o alone.
+// The tables of every length are built once per context (k_stage_tables:
+// forward then inverse, 2^l words each, lengths 2^1 .. 2^12 back to back
+// from word 2^(l+1) - 4) and each CTA copies the two it needs.
+template <int LOG_L>
+__device__ __forceinline__ constexpr uint32_t tw_off(int s) {
+  return (1u << LOG_L) - ((1u << LOG_L) >> s);
+}
+PICO_HD uint32_t tw_swz_l(uint32_t l, uint32_t x) { return l >= 9 ? x ^ ((x >> 4) & ((1u << (l - 8)) - 1u)) : x; }
+template <int LOG_L>
+__device__ __forceinline__ uint32_t tw_swz(uint32_t x) {
+  return tw_swz_l(LOG_L, x);
+}
+PICO_HD constexpr uint32_t stage_base(uint32_t l) { return (2u << l) - 4u; }
+static_assert(stage_base(13) <= kStageTableWords, "stage tables fit");
+
+template <int LOG_L>
+__device__ __forceinline__ void load_twiddles(uint32_t* dst, const TwiddleTables& tw, bool inv) {
+  const uint32_t* src = tw.stage + stage_base(LOG_L) + (inv ? (1u << LOG_L) : 0u);
+  if constexpr (LOG_L >= 2) {
+    for (uint32_t i = threadIdx.x; i < (1u << LOG_L) / 4; i += kThreads)
+      reinterpret_cast<uint4*>(dst)[i] = __ldg(reinterpret_cast<const uint4*>(src) + i);
+  } else {
+    if (threadIdx.x < (1u << LOG_L)) dst[threadIdx.x] = __ldg(src + threadIdx.x);
+  }
+}
+
+// One word of the stage tables: length 2^l (l = 1..12), direction, stage s,
+// entry x at its swizzled position; the last word of each table is unused.
+template <class F>
+__global__ void k_stage_tables(const __grid_constant__ TwiddleTables tw, uint32_t* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= stage_base(kMaxLogL + 1)) return;
+  uint32_t l = 1;
+  while (stage_base(l + 1) <= i) l++;
+  const uint32_t L = 1u << l;
+  uint32_t r = i - stage_base(l);
+  const bool inv = r >= L;
+  if (inv) r -= L;
+  uint32_t v = 0;
+  if (r < L - 1) {
+    uint32_t s = 0;
+    while (r >= L - (L >> (s + 1))) s++;
+    uint32_t x = r - (L - (L >> s));
+    if (s < 4) x = tw_swz_l(l, x);  // the swizzle is its own inverse
+    v = omega<F>(tw, l, x << s, inv);
+  }
+  out[i] = v;
 }
 
 // Swizzled shared-memory index of (position, line).  With 32 or more lines
@@ -163,12 +244,15 @@ __device__ __forceinline__ void fill_twiddles(uint32_t* t, bool inv, const Twidd
 // distinct banks for l <= 12.
 template <int LOG_LW>
 __device__ __forceinline__ uint32_t sidx(uint32_t pos, uint32_t line) {
+  uint32_t r;
   if constexpr (LOG_LW >= 5) {
-    return (pos << LOG_LW) + line;
+    r = (pos << LOG_LW) + line;
   } else {
     constexpr int SH = LOG_LW == 0 ? 5 : 4;
-    return ((pos ^ ((pos >> SH) & 15u)) << LOG_LW) + line;
+    r = ((pos ^ ((pos >> SH) & 15u)) << LOG_LW) + line;
   }
+  if (r >= s_smem_words) { guard_trip(kGuardTile, r, s_smem_words); r = 0; }
+  return r;
 }
 
 // DIF butterfly: (a, b) -> (a + b, (a - b) * w), canonical in and out.
@@ -183,20 +267,24 @@ __device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t w) {
 }
 
 // Stages S0 .. S0+R-1 of a 2^LOG_L-point DIF on v[k] = x[base + k * stride],
-// stride = L >> (S0 + R), base = blk * (L >> S0) + o;  tw[t] = w_L^(+-t).
-// The twiddle of stage s at position x is w_L^((x mod (L >> (s+1))) << s).
+// stride = L >> (S0 + R), base = blk * (L >> S0) + o;  tw = the per-stage
+// tables above.  The twiddle of stage s at position x is
+// w_L^((x mod (L >> (s+1))) << s), and x mod (L >> (s+1)) = o + (k mod half) * stride.
 template <class F, int LOG_L, int S0, int R>
 __device__ __forceinline__ void dif(uint32_t* v, uint32_t o, const uint32_t* tw) {
   constexpr int N = 1 << R;
+  constexpr uint32_t stride = 1u << (LOG_L - S0 - R);
+  static_assert(S0 == 0 || S0 >= 4 || LOG_L < 9, "swizzled stage tables are read by first rounds only");
+  const uint32_t* tb = tw + (S0 == 0 ? tw_swz<LOG_L>(o) : o);
 #pragma unroll
   for (int t = 0; t < R; t++) {
     const int half = N >> (t + 1);
-    const uint32_t obase = o << (S0 + t);
-    const uint32_t kstep = (1u << LOG_L) >> (R - t);
 #pragma unroll
     for (int k = 0; k < N; k++) {
       if (k & half) continue;
-      bfly<F>(v[k], v[k + half], tw[obase + (uint32_t)(k & (half - 1)) * kstep]);
+      uint32_t ti = (uint32_t)(tb - tw) + tw_off<LOG_L>(S0 + t) + (uint32_t)(k & (half - 1)) * stride;
+      if (ti >= (1u << LOG_L)) { guard_trip(kGuardTwiddle, ti, 1u << LOG_L); ti = 0; }
+      bfly<F>(v[k], v[k + half], tw[ti]);
     }
   }
 }
@@ -235,13 +323,16 @@ __device__ __forceinline__ void round_smem(uint32_t* buf, const uint32_t* tw) {
   }
 }
 
-// Round plan.  Inverse: a short first round (l mod 4 stages), then rounds of
-// four; the last is stride 1 and stays in registers.  Forward: the fused
-// first round of four, rounds of four, one short round, then a last round of
-// four at stride 1 (for l < 8 the short round is the last).
-template <int LOG_L>
-constexpr int inv_first_r() {
-  return LOG_L <= 4 ? LOG_L : (LOG_L % 4 ? LOG_L % 4 : 4);
+// Round plan.  Inverse: a first round of four, one short round (l mod 4
+// stages), rounds of four, and a last round of four at stride 1 that stays
+// in registers (for l < 8: the short round, then the last).  Forward: the
+// fused first round of four, rounds of four, one short round, then a last
+// round of four at stride 1 (for l < 8 the short round is the last).  Only
+// first rounds touch stages 0..3.
+template <int LOG_L, int S0>
+constexpr int inv_round_r() {
+  if constexpr (LOG_L < 8) return S0 == 0 ? LOG_L - 4 : 4;
+  return (S0 == 4 && LOG_L % 4) ? LOG_L % 4 : 4;
 }
 template <int LOG_L>
 constexpr int fwd_last_r() {
@@ -251,9 +342,10 @@ constexpr int fwd_last_r() {
 template <class F, int LOG_L, int S0>
 __device__ __forceinline__ void inv_middle(uint32_t* buf, const uint32_t* tw) {
   if constexpr (S0 + 4 < LOG_L) {
-    round_smem<F, LOG_L, S0, 4>(buf, tw);
+    constexpr int R = inv_round_r<LOG_L, S0>();
+    round_smem<F, LOG_L, S0, R>(buf, tw);
     __syncthreads();
-    inv_middle<F, LOG_L, S0 + 4>(buf, tw);
+    inv_middle<F, LOG_L, S0 + R>(buf, tw);
   }
 }
 template <class F, int LOG_L, int S0>
@@ -335,7 +427,7 @@ __device__ __forceinline__ void load_set(uint32_t* v, const uint32_t* p, uint32_
     p += (uint64_t)o * pos_step;
     const uint64_t step = pos_step << LOG_STRIDE;
 #pragma unroll
-    for (int k = 0; k < (1 << R); k++) v[k] = __ldg(p + k * step);
+    for (int k = 0; k < (1 << R); k++) v[k] = in_range(p + k * step, s_in, kGuardLoad) ? __ldg(p + k * step) : 0u;
     if constexpr (Twist::active) {
       const uint2 aq = twist(o, line, (uint32_t)LOG_STRIDE);
       uint32_t cur = aq.x;
@@ -383,9 +475,10 @@ __device__ __forceinline__ void inverse_to_regs(uint32_t* buf, const uint32_t* t
   G::item(threadIdx.x, line, o, base);
   q = base >> RL;
   if constexpr (SL > 0) {
-    first_round_global<F, LOG_L, inv_first_r<LOG_L>()>(buf, twi, line_base, pos_step, twist);
+    constexpr int R0 = inv_round_r<LOG_L, 0>();
+    first_round_global<F, LOG_L, R0>(buf, twi, line_base, pos_step, twist);
     __syncthreads();
-    inv_middle<F, LOG_L, inv_first_r<LOG_L>()>(buf, twi);
+    inv_middle<F, LOG_L, R0>(buf, twi);
 #pragma unroll
     for (int k = 0; k < (1 << RL); k++) coef[k] = buf[sidx<G::LOG_LW>(base + (uint32_t)k, line)];
   } else {
@@ -436,19 +529,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
   extern __shared__ uint32_t smem[];
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassSmall, blockIdx.x, local);
+  s_in = GuardRange{M.in, M.in + (((uint64_t)M.w << M.log_n))};
+  s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
   const TileCtx T = tile_ctx(pass_geom(M, kPassSmall), local, M.w);
   const uint32_t w = M.w;
   if constexpr (LOG_L == 0) {
     // height 1: every LDE row equals the input row (the scale g^0 / 1 is 1)
     uint32_t col, sub;
     if (line_at(T, threadIdx.x, col, sub))
-      for (uint32_t cb = 0; cb < (1u << M.log_b); cb++) M.out[(uint64_t)cb * w + col] = __ldg(M.in + col);
+      for (uint32_t cb = 0; cb < (1u << M.log_b); cb++) {
+        const uint32_t* pi = M.in + col;
+        uint32_t* po = M.out + (uint64_t)cb * w + col;
+        if (pi < M.in || pi >= M.in + w) { guard_trip(kGuardLoad, col, w); continue; }
+        if (po < M.out || po >= M.out + ((uint64_t)w << M.log_b)) { guard_trip(kGuardStore, (uint64_t)cb * w + col, (uint64_t)w << M.log_b); continue; }
+        *po = __ldg(pi);
+      }
   } else {
     uint32_t* buf = smem;
     uint32_t* twf = buf + (L << LOG_LW);
-    uint32_t* twi = twf + (L >> 1) + 1;
-    fill_twiddles<F, LOG_L>(twf, false, tw);
-    fill_twiddles<F, LOG_L>(twi, true, tw);
+    uint32_t* twi = twf + L;
+    load_twiddles<LOG_L>(twf, tw, false);
+    load_twiddles<LOG_L>(twi, tw, true);
     __syncthreads();
     auto line_base = [&](uint32_t line) -> const uint32_t* {
       uint32_t col, sub;
@@ -472,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
             if (!line_at(T, ln, col, sub)) return;
             uint32_t* p = outb + (uint64_t)base * w + col;
 #pragma unroll
-            for (int k = 0; k < (1 << RL); k++) p[(uint64_t)k * w] = v[k];
+            for (int k = 0; k < (1 << RL); k++) if (in_range(p + (uint64_t)k * w, s_out, kGuardStore)) p[(uint64_t)k * w] = v[k];
           });
     }
   }
@@ -487,11 +589,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_a(const __grid_constant__ L
   extern __shared__ uint32_t smem[];
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassA, blockIdx.x, local);
+  s_in = GuardRange{M.in, M.in + (((uint64_t)M.w << M.log_n))};
+  s_out = GuardRange{M.t1, M.t1 + (((uint64_t)M.w << M.log_n))};
+  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
   const TileCtx T = tile_ctx(pass_geom(M, kPassA), local, M.w);
   const uint32_t w = M.w, log_n2 = M.log_n2;
   uint32_t* buf = smem;
   uint32_t* twi = buf + (L << LOG_LW);
-  fill_twiddles<F, LOG_L>(twi, true, tw);
+  load_twiddles<LOG_L>(twi, tw, true);
   __syncthreads();
   auto line_base = [&](uint32_t line) -> const uint32_t* {
     uint32_t col, sub;
@@ -506,14 +611,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_a(const __grid_constant__ L
     uint32_t* p = M.t1 + ((((uint64_t)k1_0 << log_n2) + j2) * w + col);
     const uint64_t step = ((uint64_t)w << log_n2) << (LOG_L - 4);
 #pragma unroll
-    for (int kr = 0; kr < 16; kr++) p[kr * step] = coef[rev_bits(kr, 4)];
+    for (int kr = 0; kr < 16; kr++) if (in_range(p + kr * step, s_out, kGuardStore)) p[kr * step] = coef[rev_bits(kr, 4)];
   }
 }
 
 // Pass B: T1 rows k1 * n2 + j2 times w_n^-(j2 k1) -> coefficients -> per
 // coset -> T2 (the twiddle w_n^(k1 k1') is applied by pass C on its loads).
 template <class F, int LOG_L>
-__global__ void __launch_bounds__(kThreads, 1) k_lde_b(const __grid_constant__ LdeBatch batch,
+__global__ void __launch_bounds__(kThreads, 2) k_lde_b(const __grid_constant__ LdeBatch batch,
                                                        const __grid_constant__ TwiddleTables tw) {
   constexpr int LOG_LW = (int)tile_log_lw(LOG_L);
   constexpr uint32_t L = 1u << LOG_L;
@@ -521,14 +626,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_b(const __grid_constant__ L
   extern __shared__ uint32_t smem[];
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassB, blockIdx.x, local);
+  s_in = GuardRange{M.t1, M.t1 + (((uint64_t)M.w << M.log_n))};
+  s_out = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
   const TileCtx T = tile_ctx(pass_geom(M, kPassB), local, M.w);
   const uint32_t w = M.w, log_n1 = M.log_n1;
   const uint64_t n = 1ull << M.log_n;
   uint32_t* buf = smem;
   uint32_t* twf = buf + (L << LOG_LW);
-  uint32_t* twi = twf + (L >> 1) + 1;
-  fill_twiddles<F, LOG_L>(twf, false, tw);
-  fill_twiddles<F, LOG_L>(twi, true, tw);
+  uint32_t* twi = twf + L;
+  load_twiddles<LOG_L>(twf, tw, false);
+  load_twiddles<LOG_L>(twi, tw, true);
   __syncthreads();
   auto line_base = [&](uint32_t line) -> const uint32_t* {
     uint32_t col, sub;
@@ -556,7 +664,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_b(const __grid_constant__ L
           uint32_t* p = t2 + ((((uint64_t)k1p_0 << log_n1) + k1) * w + col);
           const uint64_t step2 = ((uint64_t)w << log_n1) << (LOG_L - RL);
 #pragma unroll
-          for (int kr = 0; kr < (1 << RL); kr++) p[kr * step2] = v[rev_bits(kr, RL)];
+          for (int kr = 0; kr < (1 << RL); kr++) if (in_range(p + kr * step2, s_out, kGuardStore)) p[kr * step2] = v[rev_bits(kr, RL)];
         });
   }
 }
@@ -573,6 +681,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
   extern __shared__ uint32_t smem[];
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassC, blockIdx.x, local);
+  s_in = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
   const PassGeom g = pass_geom(M, kPassC);
   const TileCtx T = tile_ctx(g, local, M.w);
   const uint32_t w = M.w, log_n2 = M.log_n2;
@@ -580,7 +691,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
   const uint64_t n = 1ull << M.log_n;
   uint32_t* buf = smem;
   uint32_t* twf = buf + (L << LOG_LW);
-  fill_twiddles<F, LOG_L>(twf, false, tw);
+  load_twiddles<LOG_L>(twf, tw, false);
   __syncthreads();
   const uint32_t* src = M.t2 + (uint64_t)cb * n * w;
   uint32_t* dst = M.out + (uint64_t)cb * n * w;
@@ -598,7 +709,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
     const uint64_t row = ((uint64_t)(__brev(k1p) >> (32 - log_n2)) << LOG_L) + base;
     uint32_t* p = dst + row * w + col;
 #pragma unroll
-    for (int k = 0; k < (1 << RL); k++) p[(uint64_t)k * w] = v[k];
+    for (int k = 0; k < (1 << RL); k++) if (in_range(p + (uint64_t)k * w, s_out, kGuardStore)) p[(uint64_t)k * w] = v[k];
   });
 }
 
@@ -622,6 +733,7 @@ __global__ void k_pow_tables(const __grid_constant__ LdeBatch batch, const __gri
   } else {
     v = B::pow(g, (uint64_t)(e - 4096u) << 12);
   }
+  if (i >= (kPwWords << M.log_b)) { guard_trip(kGuardStore, i, kPwWords << M.log_b); return; }
   M.pw[i] = v;
 }
 
@@ -635,11 +747,12 @@ void plan_lde_tiling(LdeMat& m) {
 }
 
 // Dynamic shared memory of a pass at sub-transform length 2^log_L (bytes):
-// the tile plus one (passes A, C) or two (one-pass, B) twiddle tables.
+// the tile plus one (passes A, C) or two (one-pass, B) twiddle tables of L
+// words (L - 1 used).
 static size_t smem_bytes(uint32_t log_L, int pass) {
   const size_t L = 1ull << log_L;
   const size_t tile = L << tile_log_lw(log_L);
-  const size_t tw_words = (pass == kPassA || pass == kPassC) ? L / 2 + 1 : L + 2;
+  const size_t tw_words = (pass == kPassA || pass == kPassC) ? L : 2 * L;
   return (tile + tw_words) * 4;
 }
 
@@ -736,6 +849,23 @@ static cudaError_t launch_lde_t(const LdeMat* mats, uint32_t n_mats, TwiddleTabl
     }
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_stage_tables(int field, TwiddleTables tw, uint32_t* stage, cudaStream_t st) {
+  const uint32_t n = stage_base(kMaxLogL + 1);
+  if (field == 0)
+    k_stage_tables<KoalaBear><<<(n + 255) / 256, 256, 0, st>>>(tw, stage);
+  else
+    k_stage_tables<BabyBear><<<(n + 255) / 256, 256, 0, st>>>(tw, stage);
+  return cudaGetLastError();
+}
+
+cudaError_t lde_guard_fetch(GuardRecord* dst, cudaStream_t st) {
+  return cudaMemcpyFromSymbolAsync(dst, g_lde_guard, sizeof(GuardRecord), 0, cudaMemcpyDeviceToHost, st);
+}
+cudaError_t lde_guard_clear() {
+  const GuardRecord z{};
+  return cudaMemcpyToSymbol(g_lde_guard, &z, sizeof z);
 }
 
 cudaError_t launch_lde(int field, const LdeMat* mats, uint32_t n_mats, TwiddleTables tw, cudaStream_t st,

@@ -42,8 +42,22 @@ __global__ void k_permute(uint32_t* states, uint64_t n) {
 // Absorb row r of the concatenated group into a zeroed sponge state
 // (PaddingFreeSponge<_,16,8,8>: overwrite s[0..k) with each chunk of up to 8
 // elements, permute after each chunk; hash.rs:40-52).
+// Bounds guard of the row hashing: every read is checked against its
+// segment (index, column, row); a read outside is skipped (as zero) and the
+// first one recorded in g_hash_guard, which the entry points copy back with
+// their final synchronisation and report as an error.
+__device__ GuardRecord g_hash_guard;
+__device__ __noinline__ void hash_guard_trip(unsigned long long seg, unsigned long long col) {
+  if (atomicAdd(&g_hash_guard.count, 1ull) == 0) {
+    g_hash_guard.tag = kGuardRowRead;
+    g_hash_guard.offset = seg;
+    g_hash_guard.extent = col;
+    g_hash_guard.block = blockIdx.x;
+    g_hash_guard.thread = threadIdx.x;
+  }
+}
 template <class F>
-__device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t s[16]) {
+__device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t s[16], uint64_t rows) {
   const uint32_t W = g.total_width;
   uint32_t seg = 0, col = 0;
   uint32_t segw = g.segs[0].width;
@@ -58,7 +72,8 @@ __device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t
           segw = g.segs[seg].width;
           rowp = g.segs[seg].ptr + r * segw;
         }
-        s[j] = __ldg(rowp + col);
+        if (seg >= g.n_segs || col >= segw || r >= rows) { hash_guard_trip(seg, col); s[j] = 0; }
+        else s[j] = __ldg(rowp + col);
         col++;
       }
     }
@@ -79,7 +94,7 @@ __global__ void __launch_bounds__(256) k_hash_rows(const __grid_constant__ RowGr
   uint32_t s[16];
 #pragma unroll
   for (int i = 0; i < 16; i++) s[i] = 0;
-  hash_row<F>(g, r, s);
+  hash_row<F>(g, r, s, rows);
   store_digest(out + 8 * r, s);
 }
 
@@ -129,6 +144,14 @@ cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t
   else
     k_permute<BabyBear><<<blocks_for(n, 256), 256, 0, st>>>(states, n);
   return cudaGetLastError();
+}
+
+cudaError_t hash_guard_fetch(GuardRecord* dst, cudaStream_t st) {
+  return cudaMemcpyFromSymbolAsync(dst, g_hash_guard, sizeof(GuardRecord), 0, cudaMemcpyDeviceToHost, st);
+}
+cudaError_t hash_guard_clear() {
+  const GuardRecord z{};
+  return cudaMemcpyToSymbol(g_hash_guard, &z, sizeof z);
 }
 
 cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st) {

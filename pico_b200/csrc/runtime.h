@@ -61,12 +61,18 @@ struct Server;  // serving.h
 
 bool try_reserve(pico_ctx* ctx, uint64_t bytes);
 void unreserve(pico_ctx* ctx, uint64_t bytes);
-cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr, cudaStream_t* lde_stream = nullptr);
+cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr, uint32_t* slot = nullptr);
 cudaStream_t aux_stream(pico_ctx* ctx);
 TwiddleTables twiddles(pico_ctx* ctx, int field);
 pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
-                           cudaStream_t lst, pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
+                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
 void free_commit_buffers(pico_commit* c, cudaStream_t st);
+// Bounds guards of the kernels (GuardRecord): guard_enqueue copies both
+// units' records into the slot's pinned host records on st; after st has
+// been synchronised, guard_verdict returns PICO_OK, or an error naming the
+// first skipped access (and clears the device records).
+pico_status guard_enqueue(pico_ctx* ctx, uint32_t slot, cudaStream_t st);
+pico_status guard_verdict(pico_ctx* ctx, uint32_t slot, std::string* msg = nullptr);
 pico_status finish_stats(pico_commit* c);
 
 }  // namespace pico
@@ -80,11 +86,11 @@ struct pico_ctx {
   std::condition_variable cv;  // signalled whenever reserved memory is returned
   std::vector<cudaStream_t> streams;
   std::vector<cudaStream_t> copy_streams;  // paired with streams[i]: host -> device input copies
-  std::vector<cudaStream_t> lde_streams;   // paired with streams[i]: LDE kernels
   std::atomic<uint32_t> next_stream{0};
   std::vector<cudaStream_t> aux_streams;  // read-backs and releases of finished work
   std::atomic<uint32_t> next_aux{0};
-  uint32_t* tw[2] = {nullptr, nullptr};  // per-field twiddle tables (lo | hi)
+  uint32_t* tw[2] = {nullptr, nullptr};  // per-field twiddle tables (lo | hi | stage)
+  pico::GuardRecord* guard_host = nullptr;  // pinned: 2 records (LDE, hashing) per stream slot
   pico::Server* server = nullptr;
   ~pico_ctx();
 };
@@ -102,8 +108,11 @@ struct pico_commit {
   uint32_t* layers = nullptr;     // all digest layers, leaves first
   uint64_t bytes_resident = 0;
   uint32_t root[8] = {0};
-  // events (see finish_stats): compute-stream phases 0..4, copy stream 5..6
+  // events (see finish_stats): compute-stream phases 0, 3, 4, copy stream 5..6,
+  // and four per height group around its LDE and its row hashing
   cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> group_ev;
+  void destroy_events();
   pico_commit_stats stats{};
   ~pico_commit();
 };

@@ -15,6 +15,7 @@
 //   - LDEs and digest layers stay resident (and budgeted) until the caller
 //     releases the commit handed over by pico_gpu_wait.
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <list>
 
@@ -64,6 +65,16 @@ static void CUDART_CB on_request_done(void* arg) {
   std::lock_guard<std::mutex> g(sv->mu);
   memcpy(r->root, r->root_pinned, 32);
   memcpy(r->commit->root, r->root_pinned, 32);
+  // bounds guards (host memory only here: no CUDA calls in a stream callback;
+  // the device records stay set until a synchronous call reports and clears them)
+  const GuardRecord* gr = r->ctx->guard_host + 2 * r->slot;
+  if (gr[0].count || gr[1].count) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "internal bounds guard: %s kernel skipped an access (tag %llu)",
+             gr[0].count ? "LDE" : "row hashing", gr[0].count ? gr[0].tag : gr[1].tag);
+    r->status = PICO_ERR_CUDA;
+    r->error = buf;
+  }
   r->t_done = Clock::now();
   r->state = pico_request::DONE;
   sv->slot_busy[r->slot] = false;
@@ -97,14 +108,12 @@ static void launch_request(Server* sv, pico_request* r) {
   pico_ctx* ctx = sv->ctx;
   cudaStream_t st = ctx->streams[r->slot];
   r->commit = new pico_commit();
-  pico_status s = enqueue_commit(ctx, r->plan, st, ctx->copy_streams[r->slot], ctx->lde_streams[r->slot], r->commit,
-                                 r->scratch, r->root_pinned);
-  if (s) {  // copies and LDEs may still target scratch
-    cudaStreamSynchronize(ctx->copy_streams[r->slot]);
-    cudaStreamSynchronize(ctx->lde_streams[r->slot]);
-  }
+  pico_status s = enqueue_commit(ctx, r->plan, st, ctx->copy_streams[r->slot], r->commit, r->scratch,
+                                 r->root_pinned);
+  if (s) cudaStreamSynchronize(ctx->copy_streams[r->slot]);  // copies may still target scratch
   for (void* p : r->scratch) cudaFreeAsync(p, st);
   r->scratch.clear();
+  if (s == PICO_OK) s = guard_enqueue(ctx, r->slot, st);
   if (s == PICO_OK) s = cuda_status(cudaLaunchHostFunc(st, on_request_done, r), "completion callback");
   if (s != PICO_OK) {
     const std::string msg = pico_gpu_last_error();
