@@ -8,7 +8,7 @@
 // f(shift * w_N^rev(i)) (vm/src/compiler/recursion/circuit/fri.rs:155-171).
 //
 // Tiles.  A CTA of 512 threads stages a tile of L = 2^l positions x LW lines
-// in shared memory (L * LW = 2^13 words, 32 KiB, for l >= 4); a line is one
+// in shared memory (L * LW = 2^13 words, 32 KiB plus padding, for l >= 4); a line is one
 // column of one sub-transform (J adjacent sub-transforms x ws adjacent
 // columns).  The sub-transform length l is a template parameter: one launch
 // per (pass, l) group, so every stride, round size and twiddle offset is a
@@ -16,8 +16,8 @@
 // in, bit-reversed out) and run in rounds of up to four radix-2 stages held in
 // registers: a thread loads the 2^r elements a round combines, applies r
 // stages and stores them back, so shared memory sees one round trip per four
-// stages.  Positions are XOR-swizzled (low four bits with the next four) so
-// that neither strided nor stride-1 rounds conflict on banks.
+// stages.  The tile is padded (LW spare words every 16 positions) so that
+// neither strided nor stride-1 rounds conflict on banks.
 //
 // Fusion.  The inverse transform's last round works on 16 consecutive
 // positions; those 16 values are exactly the 16 inputs of the forward
@@ -237,21 +237,37 @@ __global__ void k_stage_tables(const __grid_constant__ TwiddleTables tw, uint32_
   out[i] = v;
 }
 
-// Swizzled shared-memory index of (position, line).  With 32 or more lines
-// the lines alone spread a warp over the banks; with fewer, the low four
-// position bits are XORed with the next four (the four after bit 5 with a
-// single line), which keeps every warp access of every round below on
-// distinct banks for l <= 12.
+// Shared-memory layout of a tile: position-major, LW lines per position.
+// With fewer than 32 lines, LW spare words follow every 16 positions (word
+// (pos + pos/16) * LW + line), which puts every warp access of every round
+// below on distinct banks; with 32 or more lines the lines alone do.  Within
+// a set of a round the positions are base + k * stride with stride a multiple
+// of 16, or stride 1 from a base aligned to the set, so the padded words are
+// row + k * step: one address computation per set, the rest immediates.
+PICO_HD constexpr uint32_t tile_words_l(uint32_t l) {
+  return ((1u << l) + (tile_log_lw(l) < 5 ? (1u << l) >> 4 : 0u)) << tile_log_lw(l);
+}
 template <int LOG_LW>
-__device__ __forceinline__ uint32_t sidx(uint32_t pos, uint32_t line) {
-  uint32_t r;
+__device__ __forceinline__ uint32_t srow(uint32_t pos, uint32_t line) {
   if constexpr (LOG_LW >= 5) {
-    r = (pos << LOG_LW) + line;
+    return (pos << LOG_LW) + line;
   } else {
-    constexpr int SH = LOG_LW == 0 ? 5 : 4;
-    r = ((pos ^ ((pos >> SH) & 15u)) << LOG_LW) + line;
+    return ((pos + (pos >> 4)) << LOG_LW) + line;
   }
-  if (r >= s_smem_words) { guard_trip(kGuardTile, r, s_smem_words); r = 0; }
+}
+template <int LOG_LW, int LOG_STRIDE>
+__device__ __forceinline__ constexpr uint32_t sstep() {
+  return (LOG_LW >= 5 || LOG_STRIDE < 4 ? (1u << LOG_STRIDE) : (1u << LOG_STRIDE) + (1u << (LOG_STRIDE - 4)))
+         << LOG_LW;
+}
+// Row of a set of N elements; the guard checks the set's last word.
+template <int LOG_LW, int LOG_STRIDE, int N>
+__device__ __forceinline__ uint32_t set_row(uint32_t pos, uint32_t line) {
+  uint32_t r = srow<LOG_LW>(pos, line);
+  if (r + (uint32_t)(N - 1) * sstep<LOG_LW, LOG_STRIDE>() >= s_smem_words) {
+    guard_trip(kGuardTile, r, s_smem_words);
+    r = 0;
+  }
   return r;
 }
 
@@ -315,11 +331,13 @@ __device__ __forceinline__ void round_smem(uint32_t* buf, const uint32_t* tw) {
     uint32_t line, o, base;
     G::item(threadIdx.x + j * kThreads, line, o, base);
     uint32_t v[1 << R];
+    constexpr uint32_t ST = sstep<G::LOG_LW, G::LOG_STRIDE>();
+    uint32_t* row = buf + set_row<G::LOG_LW, G::LOG_STRIDE, (1 << R)>(base, line);
 #pragma unroll
-    for (int k = 0; k < (1 << R); k++) v[k] = buf[sidx<G::LOG_LW>(base + ((uint32_t)k << G::LOG_STRIDE), line)];
+    for (int k = 0; k < (1 << R); k++) v[k] = row[k * ST];
     dif<F, LOG_L, S0, R>(v, o, tw);
 #pragma unroll
-    for (int k = 0; k < (1 << R); k++) buf[sidx<G::LOG_LW>(base + ((uint32_t)k << G::LOG_STRIDE), line)] = v[k];
+    for (int k = 0; k < (1 << R); k++) row[k * ST] = v[k];
   }
 }
 
@@ -371,8 +389,10 @@ __device__ __forceinline__ void fwd_last(const uint32_t* buf, const uint32_t* tw
     uint32_t line, o, base;
     G::item(threadIdx.x + j * kThreads, line, o, base);
     uint32_t v[1 << RL];
+    constexpr uint32_t ST = sstep<G::LOG_LW, 0>();
+    const uint32_t* row = buf + set_row<G::LOG_LW, 0, (1 << RL)>(base, line);
 #pragma unroll
-    for (int k = 0; k < (1 << RL); k++) v[k] = buf[sidx<G::LOG_LW>(base + (uint32_t)k, line)];
+    for (int k = 0; k < (1 << RL); k++) v[k] = row[k * ST];
     dif<F, LOG_L, SL, RL>(v, 0u, tw);
     store(line, base, v);
   }
@@ -455,8 +475,10 @@ __device__ __forceinline__ void first_round_global(uint32_t* buf, const uint32_t
     uint32_t v[1 << R];
     load_set<F, R, G::LOG_STRIDE>(v, line_base(line), o, line, pos_step, twist);
     dif<F, LOG_L, 0, R>(v, o, tw);
+    constexpr uint32_t ST = sstep<G::LOG_LW, G::LOG_STRIDE>();
+    uint32_t* row = buf + set_row<G::LOG_LW, G::LOG_STRIDE, (1 << R)>(base, line);
 #pragma unroll
-    for (int k = 0; k < (1 << R); k++) buf[sidx<G::LOG_LW>(base + ((uint32_t)k << G::LOG_STRIDE), line)] = v[k];
+    for (int k = 0; k < (1 << R); k++) row[k * ST] = v[k];
   }
 }
 
@@ -479,8 +501,10 @@ __device__ __forceinline__ void inverse_to_regs(uint32_t* buf, const uint32_t* t
     first_round_global<F, LOG_L, R0>(buf, twi, line_base, pos_step, twist);
     __syncthreads();
     inv_middle<F, LOG_L, R0>(buf, twi);
+    constexpr uint32_t ST = sstep<G::LOG_LW, 0>();
+    const uint32_t* row = buf + set_row<G::LOG_LW, 0, (1 << RL)>(base, line);
 #pragma unroll
-    for (int k = 0; k < (1 << RL); k++) coef[k] = buf[sidx<G::LOG_LW>(base + (uint32_t)k, line)];
+    for (int k = 0; k < (1 << RL); k++) coef[k] = row[k * ST];
   } else {
     load_set<F, RL, 0>(coef, line_base(line), 0u, line, pos_step, twist);
   }
@@ -511,8 +535,10 @@ __device__ __forceinline__ void forward_from_regs(uint32_t* buf, const uint32_t*
     store(line, 0u, v);
   } else {
     __syncthreads();  // shared memory may still be read by the previous phase
+    constexpr uint32_t ST = sstep<G::LOG_LW, LOG_STRIDE>();
+    uint32_t* row = buf + set_row<G::LOG_LW, LOG_STRIDE, (1 << RF)>(o, line);
 #pragma unroll
-    for (int k = 0; k < (1 << RF); k++) buf[sidx<G::LOG_LW>(o + ((uint32_t)k << LOG_STRIDE), line)] = v[k];
+    for (int k = 0; k < (1 << RF); k++) row[k * ST] = v[k];
     __syncthreads();
     fwd_middle<F, LOG_L, RF>(buf, twf);
     fwd_last<F, LOG_L>(buf, twf, store);
@@ -531,7 +557,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
   const LdeMat& M = find_tile(batch, kPassSmall, blockIdx.x, local);
   s_in = GuardRange{M.in, M.in + (((uint64_t)M.w << M.log_n))};
   s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + M.log_b)))};
-  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
+  s_smem_words = tile_words_l(LOG_L);
   const TileCtx T = tile_ctx(pass_geom(M, kPassSmall), local, M.w);
   const uint32_t w = M.w;
   if constexpr (LOG_L == 0) {
@@ -547,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
       }
   } else {
     uint32_t* buf = smem;
-    uint32_t* twf = buf + (L << LOG_LW);
+    uint32_t* twf = buf + tile_words_l(LOG_L);
     uint32_t* twi = twf + L;
     load_twiddles<LOG_L>(twf, tw, false);
     load_twiddles<LOG_L>(twi, tw, true);
@@ -585,17 +611,16 @@ template <class F, int LOG_L>
 __global__ void __launch_bounds__(kThreads, 2) k_lde_a(const __grid_constant__ LdeBatch batch,
                                                        const __grid_constant__ TwiddleTables tw) {
   constexpr int LOG_LW = (int)tile_log_lw(LOG_L);
-  constexpr uint32_t L = 1u << LOG_L;
   extern __shared__ uint32_t smem[];
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassA, blockIdx.x, local);
   s_in = GuardRange{M.in, M.in + (((uint64_t)M.w << M.log_n))};
   s_out = GuardRange{M.t1, M.t1 + (((uint64_t)M.w << M.log_n))};
-  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
+  s_smem_words = tile_words_l(LOG_L);
   const TileCtx T = tile_ctx(pass_geom(M, kPassA), local, M.w);
   const uint32_t w = M.w, log_n2 = M.log_n2;
   uint32_t* buf = smem;
-  uint32_t* twi = buf + (L << LOG_LW);
+  uint32_t* twi = buf + tile_words_l(LOG_L);
   load_twiddles<LOG_L>(twi, tw, true);
   __syncthreads();
   auto line_base = [&](uint32_t line) -> const uint32_t* {
@@ -628,12 +653,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_b(const __grid_constant__ L
   const LdeMat& M = find_tile(batch, kPassB, blockIdx.x, local);
   s_in = GuardRange{M.t1, M.t1 + (((uint64_t)M.w << M.log_n))};
   s_out = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + M.log_b)))};
-  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
+  s_smem_words = tile_words_l(LOG_L);
   const TileCtx T = tile_ctx(pass_geom(M, kPassB), local, M.w);
   const uint32_t w = M.w, log_n1 = M.log_n1;
   const uint64_t n = 1ull << M.log_n;
   uint32_t* buf = smem;
-  uint32_t* twf = buf + (L << LOG_LW);
+  uint32_t* twf = buf + tile_words_l(LOG_L);
   uint32_t* twi = twf + L;
   load_twiddles<LOG_L>(twf, tw, false);
   load_twiddles<LOG_L>(twi, tw, true);
@@ -675,7 +700,6 @@ template <class F, int LOG_L>
 __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ LdeBatch batch,
                                                        const __grid_constant__ TwiddleTables tw) {
   constexpr int LOG_LW = (int)tile_log_lw(LOG_L);
-  constexpr uint32_t L = 1u << LOG_L;
   constexpr int RL = fwd_last_r<LOG_L>();
   static_assert(LOG_L > 4, "three-pass sub-transforms have at least 2^6 points");
   extern __shared__ uint32_t smem[];
@@ -683,14 +707,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
   const LdeMat& M = find_tile(batch, kPassC, blockIdx.x, local);
   s_in = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + M.log_b)))};
   s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + M.log_b)))};
-  s_smem_words = (uint32_t)(((1u << LOG_L) << tile_log_lw(LOG_L)));
+  s_smem_words = tile_words_l(LOG_L);
   const PassGeom g = pass_geom(M, kPassC);
   const TileCtx T = tile_ctx(g, local, M.w);
   const uint32_t w = M.w, log_n2 = M.log_n2;
   const uint32_t cb = local / (g.n_ct * g.groups);
   const uint64_t n = 1ull << M.log_n;
   uint32_t* buf = smem;
-  uint32_t* twf = buf + (L << LOG_LW);
+  uint32_t* twf = buf + tile_words_l(LOG_L);
   load_twiddles<LOG_L>(twf, tw, false);
   __syncthreads();
   const uint32_t* src = M.t2 + (uint64_t)cb * n * w;
@@ -751,7 +775,7 @@ void plan_lde_tiling(LdeMat& m) {
 // words (L - 1 used).
 static size_t smem_bytes(uint32_t log_L, int pass) {
   const size_t L = 1ull << log_L;
-  const size_t tile = L << tile_log_lw(log_L);
+  const size_t tile = tile_words_l(log_L);
   const size_t tw_words = (pass == kPassA || pass == kPassC) ? L : 2 * L;
   return (tile + tw_words) * 4;
 }
