@@ -174,14 +174,26 @@ def barrier(world):
 
 
 def allmax(world, v: float) -> float:
+    """Max of v over the ranks (the slowest replica sets the job's time)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Each replica commits its own shard: a distinct seed per rank."""
+    return base + 7919 * rank
+
+
+def job_rate(world: int, cells_per_rank: int, steps: int, max_ms: float) -> float:
+    """Whole-job throughput: the cells every rank committed over the slowest rank's time."""
+    return world * cells_per_rank * steps / (max_ms / 1e3)
 
 
 # ---------------------------------------------------------------- CPU legs
@@ -243,7 +255,7 @@ def run_gpu(args, rank, world, local):
     wl = WORKLOADS[args.workload]
     field, b = wl["field"], wl["log_blowup"]
     shapes = wl["shapes"]()
-    seed = wl["seed"] + 7919 * rank  # each replica commits its own shard
+    seed = replica_seed(wl["seed"], rank)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     traces = [F.random_matrix_torch(field, lh, w, seed * 1000 + i, dev) for i, (lh, w) in enumerate(shapes)]
@@ -282,7 +294,7 @@ def run_gpu(args, rank, world, local):
 
     ms, stats, clocks = timed(traces)
     ms_step = ms / args.steps
-    value = world * cells * args.steps / (ms / 1e3)
+    value = job_rate(world, cells, args.steps, ms)
 
     # plain per-matrix form (the baseline form), same inputs
     ms_plain, _, _ = timed(traces, plain=True) if not args.skip_plain else (None, None, None)
