@@ -487,9 +487,13 @@ def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30):
 
 def run_serving(args):
     """Poisson arrivals of commit requests into the serving queue (admission
-    by free HBM, concurrent streams), against the same requests committed one
-    at a time (batched form, and plain one-matrix-per-launch form).  Inputs
-    are views into a device-resident pool of seeded field elements."""
+    by free HBM, up to --slots requests on the device at once), for both the
+    batched form and the plain one-matrix-per-launch form, at several offered
+    loads (multiples of the plain form's one-at-a-time capacity, the same
+    arrival times for both forms); plus both forms one at a time.  Inputs are
+    views into a device-resident pool of seeded field elements.  The memory
+    pool is grown before timing by one pass of every request, one at a time
+    and served."""
     import threading as th
 
     import torch
@@ -516,72 +520,86 @@ def run_serving(args):
     mats = [views(f, shapes, 7 * i + 1) for i, (f, b, shapes) in enumerate(reqs)]
     cells = [sum(w << lh for lh, w in shapes) for (_, _, shapes) in reqs]
     total_cells = sum(cells)
-    ctx = GpuContext(0, n_streams=8)
+    ctx = GpuContext(0, n_streams=8, max_inflight=args.slots)
+    server = CommitServer(ctx)
 
-    # one at a time: batched and plain forms
     def sequential(plain):
         lat = []
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for (f, b, shapes), m in zip(reqs, mats):
             t = time.perf_counter()
-            pcs = TwoAdicFriPcs(ctx, f, b)
-            pcs.commit([(TwoAdicDomain(lh), x) for (lh, _), x in zip(shapes, m)], plain=plain, keep=False)
+            TwoAdicFriPcs(ctx, f, b).commit([(TwoAdicDomain(lh), x) for (lh, _), x in zip(shapes, m)], plain=plain,
+                                            keep=False)
             lat.append(time.perf_counter() - t)
         return time.perf_counter() - t0, lat
 
-    warm = min(3, len(reqs))
-    for (f, b, shapes), m in list(zip(reqs, mats))[:warm]:
-        TwoAdicFriPcs(ctx, f, b).commit([(TwoAdicDomain(lh), x) for (lh, _), x in zip(shapes, m)], keep=False)
-    seq_s, seq_lat = sequential(False)
-    plain_s, plain_lat = sequential(True)
-    capacity = total_cells / seq_s
-    rate = args.load * capacity / (total_cells / len(reqs))  # requests per second
-    rng = np.random.default_rng(55)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    def served(plain, arrivals):
+        handles = [None] * len(reqs)
+        lat = [None] * len(reqs)
+        queued = [None] * len(reqs)
+        t0 = time.perf_counter()
 
-    server = CommitServer(ctx)
-    handles = [None] * len(reqs)
-    lat = [None] * len(reqs)
-    t_submit = [0.0] * len(reqs)
-    t0 = time.perf_counter()
+        def waiter():
+            for i in range(len(reqs)):
+                while handles[i] is None:
+                    time.sleep(0.0002)
+                handles[i].wait(keep=False)
+                q_us, run_us = handles[i].times()
+                lat[i] = (q_us + run_us) / 1e6
+                queued[i] = q_us / 1e6
+                handles[i].free()
 
-    def waiter():
-        for i in range(len(reqs)):
-            while handles[i] is None:
-                time.sleep(0.0002)
-            handles[i].wait(keep=False)
-            q_us, run_us = handles[i].times()
-            lat[i] = (q_us + run_us) / 1e6
-            handles[i].free()
-
-    wt = th.Thread(target=waiter)
-    wt.start()
-    for i, ((f, b, shapes), m) in enumerate(zip(reqs, mats)):
-        now = time.perf_counter() - t0
-        if arrivals[i] > now:
-            time.sleep(arrivals[i] - now)
-        t_submit[i] = time.perf_counter() - t0
-        handles[i] = server.submit(f, m, b)
-    wt.join()
-    served_s = time.perf_counter() - t0
-    ctx.close()
+        wt = th.Thread(target=waiter)
+        wt.start()
+        for i, ((f, b, shapes), m) in enumerate(zip(reqs, mats)):
+            now = time.perf_counter() - t0
+            if arrivals[i] > now:
+                time.sleep(arrivals[i] - now)
+            handles[i] = server.submit(f, m, b, plain=plain)
+        wt.join()
+        return time.perf_counter() - t0, lat, queued
 
     def pct(x, q):
         return float(np.percentile(np.array(x) * 1e3, q))
 
+    # grow the pool: every request once, one at a time, then once served back to back
+    sequential(False)
+    served(False, np.zeros(len(reqs)))
+    seq_s, seq_lat = sequential(False)
+    plain_s, plain_lat = sequential(True)
+    cap_plain = total_cells / plain_s
+    rng = np.random.default_rng(55)
+    gaps = rng.exponential(1.0, size=len(reqs))  # unit-rate arrivals, scaled per load
+    mean_cells = total_cells / len(reqs)
+    sweep = []
+    for load in sorted(set([args.load] + [0.5, 1.0, 1.25])):
+        rate = load * cap_plain / mean_cells  # requests per second
+        arrivals = np.cumsum(gaps / rate)
+        row = {"offered_load_vs_plain_capacity": load, "poisson_rate_per_s": rate}
+        for name, plain in (("batched", False), ("plain", True)):
+            s_, lat, queued = served(plain, arrivals)
+            row[name] = {"cells_per_s": total_cells / s_, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                         "mean_queue_ms": float(np.mean(queued) * 1e3)}
+        sweep.append(row)
+    ctx.close()
+    main_row = next(r for r in sweep if r["offered_load_vs_plain_capacity"] == args.load)
     return {
         "metric": "served commit throughput (trace cells/sec) with p50/p99 latency",
-        "value": total_cells / served_s, "unit": "cells/s", "n_gpus": 1, "steps": len(reqs), "warmup": warm,
-        "ms_per_step": served_s * 1e3 / len(reqs), "higher_is_better": True, "scaling": "weak",
+        "value": main_row["batched"]["cells_per_s"], "unit": "cells/s", "n_gpus": 1, "steps": len(reqs),
+        "warmup": 2 * len(reqs),
+        "ms_per_step": total_cells / main_row["batched"]["cells_per_s"] * 1e3 / len(reqs),
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic: views into a seeded device pool",
-        "config": {"workload": "serving", "requests": len(reqs), "offered_load": args.load,
-                   "poisson_rate_per_s": rate, "total_cells": total_cells},
-        "served": {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "cells_per_s": total_cells / served_s},
+        "config": {"workload": "serving", "requests": len(reqs), "slots": args.slots, "offered_load": args.load,
+                   "total_cells": total_cells},
+        "served": main_row["batched"],
+        "served_plain": main_row["plain"],
+        "sweep": sweep,
         "one_at_a_time_batched": {"p50_ms": pct(seq_lat, 50), "p99_ms": pct(seq_lat, 99),
                                   "cells_per_s": total_cells / seq_s},
         "one_at_a_time_plain": {"p50_ms": pct(plain_lat, 50), "p99_ms": pct(plain_lat, 99),
-                                "cells_per_s": total_cells / plain_s},
+                                "cells_per_s": cap_plain},
     }
 
 
@@ -593,7 +611,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving"], default="uneven-kb-2^30")
     ap.add_argument("--requests", type=int, default=60, help="serving: number of requests")
-    ap.add_argument("--load", type=float, default=0.8, help="serving: offered load vs one-at-a-time capacity")
+    ap.add_argument("--load", type=float, default=0.8,
+                    help="serving: offered load vs the plain form's one-at-a-time capacity")
+    ap.add_argument("--slots", type=int, default=2, help="serving: requests on the device at once")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")

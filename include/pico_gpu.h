@@ -78,7 +78,8 @@ typedef struct {
   uint64_t hbm_budget_bytes; /* admission budget; 0 = 90% of free HBM at init */
   uint32_t n_streams;        /* device streams for concurrent requests; 0 = 8 */
   uint32_t flags;
-  uint32_t reserved[6];
+  uint32_t max_inflight;     /* serving: requests on the device at once; 0 = n_streams */
+  uint32_t reserved[5];
 } pico_config;
 
 /* Device-side timing and work counts of one commit, from CUDA events recorded

@@ -57,7 +57,8 @@ class Config(C.Structure):
         ("hbm_budget_bytes", C.c_uint64),
         ("n_streams", C.c_uint32),
         ("flags", C.c_uint32),
-        ("reserved", C.c_uint32 * 6),
+        ("max_inflight", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
     ]
 
 

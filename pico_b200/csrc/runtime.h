@@ -92,6 +92,7 @@ struct pico_ctx {
   uint32_t* tw[2] = {nullptr, nullptr};  // per-field twiddle tables (lo | hi | stage)
   pico::GuardRecord* guard_host = nullptr;  // pinned: 2 records (LDE, hashing) per stream slot
   pico::Server* server = nullptr;
+  uint32_t max_inflight = 0;  // serving: requests on the device at once
   ~pico_ctx();
 };
 

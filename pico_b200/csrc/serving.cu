@@ -6,7 +6,8 @@
 //   - submit copies host inputs (or keeps device pointers), plans the commit
 //     and queues it; nothing touches the device on the caller's thread;
 //   - a dispatcher thread admits queued requests first-fit against the HBM
-//     budget (LDEs + digest layers + scratch) while a stream slot is free; a
+//     budget (LDEs + digest layers + scratch) while a stream slot is free and
+//     fewer than pico_config.max_inflight requests are on the device; a
 //     request that has waited longer than kStarveMs blocks later ones from
 //     overtaking it, so large requests are not starved;
 //   - each admitted request is enqueued whole on its own stream, so requests
@@ -85,13 +86,14 @@ static void CUDART_CB on_request_done(void* arg) {
 // Caller holds mu.  Claims a stream slot and the request's budget; returns
 // false (claiming nothing) if either is unavailable.
 bool Server::admit(pico_request* r) {
-  int slot = -1;
-  for (int i = 0; i < (int)slot_busy.size(); i++)
-    if (!slot_busy[i]) {
+  int slot = -1, busy = 0;
+  for (int i = 0; i < (int)slot_busy.size(); i++) {
+    if (slot_busy[i])
+      busy++;
+    else if (slot < 0)
       slot = i;
-      break;
-    }
-  if (slot < 0) return false;
+  }
+  if (slot < 0 || busy >= (int)ctx->max_inflight) return false;
   const uint64_t need = r->plan.bytes_resident + r->plan.bytes_scratch;
   if (!try_reserve(ctx, need)) return false;
   slot_busy[slot] = true;

@@ -44,11 +44,12 @@ def _log2_exact(n: int) -> int:
 class GpuContext:
     """One device context (pico_gpu_init).  Thread-safe; close() when done."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, n_streams: int = 0):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, n_streams: int = 0, max_inflight: int = 0):
         self.lib = abi.load()
         cfg = abi.Config()
         cfg.hbm_budget_bytes = hbm_budget_bytes
         cfg.n_streams = n_streams
+        cfg.max_inflight = max_inflight
         h = C.c_void_p()
         abi.check(self.lib.pico_gpu_init(device, C.byref(cfg), C.byref(h)))
         self.handle = h
@@ -360,7 +361,7 @@ class CommitServer:
     def __init__(self, ctx: GpuContext):
         self.ctx = ctx
 
-    def submit(self, field, traces, log_blowup: int, shifts=None) -> CommitRequest:
+    def submit(self, field, traces, log_blowup: int, shifts=None, plain: bool = False) -> CommitRequest:
         f = F.field_id(field)
         n = len(traces)
         mats = (abi.Matrix * n)()
@@ -368,6 +369,8 @@ class CommitServer:
         if any(dev) and not all(dev):
             raise ValueError("traces must be all host or all device")
         flags = abi.PICO_INPUT_DEVICE if all(dev) else 0
+        if plain:
+            flags |= abi.PICO_COMMIT_PLAIN
         for k, t in enumerate(traces):
             mats[k].values = _ptr(t)
             mats[k].log_height = _log2_exact(t.shape[0])
