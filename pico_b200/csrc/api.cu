@@ -363,13 +363,18 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   scr += 4096 + n * (sizeof(LdeMat) + 16);
   // Work counts: one permutation per 8 absorbed elements per row of each
   // height group, one compression per internal node, one more per injected node.
+  uint64_t state_rows = 0;  // host inputs: row states of the largest group hashed matrix by matrix
   for (size_t gi = 0; gi < plan.groups.size(); gi++) {
     uint64_t wsum = 0;
+    uint32_t nonzero = 0;
     for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) {
       wsum += plan.mats[k].w;
+      nonzero += plan.mats[k].w != 0;
       plan.lde_cells += (uint64_t)plan.mats[k].w << plan.mats[k].log_N;
     }
     const uint64_t rows = 1ull << plan.mats[plan.groups[gi].first].log_N;
+    if (gi > 0) scr += rows * 32;  // injected-row digests
+    if (!plan.input_device && nonzero >= 2) state_rows = std::max(state_rows, rows);
     const uint64_t absorb = rows * ((wsum + 7) / 8);
     if (gi == 0)
       plan.leaf_permutations = absorb;
@@ -377,6 +382,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
       plan.permutations += absorb + rows;
   }
   plan.permutations += plan.leaf_permutations + ((1ull << plan.log_max) - 1);
+  scr += state_rows * 64;
   plan.bytes_resident = res;
   plan.bytes_scratch = scr;
   return PICO_OK;
@@ -502,9 +508,33 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       }
     }
   }
+  // With host inputs, a group of several matrices is hashed one matrix at a
+  // time as each arrives (resumable sponge), the row states kept in `state`
+  // between matrices; its size is the largest such group's rows x 16 words.
+  auto nonzero = [&](uint32_t gi) {
+    uint32_t c = 0;
+    for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) c += plan.mats[k].w != 0;
+    return c;
+  };
+  std::vector<bool> chained(G, false);
+  uint32_t* state = nullptr;
+  {
+    uint64_t rows_max = 0;
+    for (uint32_t gi = 0; gi < G; gi++) {
+      chained[gi] = copy_in && nonzero(gi) >= 2;
+      if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
+    }
+    if (rows_max) {
+      void* d;
+      if ((s = alloc_async(&d, rows_max * 64, st))) return s;
+      scratch.push_back(d);
+      state = (uint32_t*)d;
+    }
+  }
 
-  // ---- host -> device copies on cst, shortest group first ----
-  std::vector<cudaEvent_t> arrived(G, nullptr);
+  // ---- host -> device copies on cst: shortest group first, each group's
+  // matrices in commit order; arrived[k] marks matrix k (and all before it) ----
+  std::vector<cudaEvent_t> arrived(n, nullptr);
   auto destroy_events = [&]() {
     for (auto e : arrived)
       if (e) cudaEventDestroy(e);  // released once the device has passed them
@@ -514,23 +544,23 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     if ((s = cuda_status(cudaStreamWaitEvent(cst, c->ev[5], 0), "copy stream wait"))) return s;
     for (uint32_t gi = G; gi-- > 0;) {
       for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) {
-        if (!in_bytes[k]) continue;
-        if ((s = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(dev_in[k]), plan.mats[k].src, in_bytes[k],
+        if (in_bytes[k] &&
+            (s = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(dev_in[k]), plan.mats[k].src, in_bytes[k],
                                              cudaMemcpyHostToDevice, cst),
                              "input copy"))) {
           destroy_events();
           return s;
         }
-      }
-      cudaEvent_t e;
-      if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) {
-        destroy_events();
-        return s;
-      }
-      arrived[gi] = e;
-      if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) {
-        destroy_events();
-        return s;
+        cudaEvent_t e;
+        if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) {
+          destroy_events();
+          return s;
+        }
+        arrived[k] = e;
+        if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) {
+          destroy_events();
+          return s;
+        }
       }
     }
     if ((s = cuda_status(cudaEventRecord(c->ev[6], cst), "event"))) {
@@ -544,14 +574,15 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   // ---- compute on st, one height group at a time ----
   // Shortest group first (the order host copies arrive in): its LDE, then
   // the digests of its rows; the tallest group's rows are the leaves and come
-  // last, then the compression levels.  Each phase of each group sits
+  // last, then the compression levels.  A chained group (host inputs, several
+  // matrices) runs matrix by matrix as each arrives: its LDE, then the
+  // absorption of its columns into the group's row states.  Each phase sits
   // between a pair of events, so the timings add up exactly.
   const TwiddleTables tw = twiddles(ctx, field);
   // Width-0 matrices add nothing to a row, so they get no segment.
-  auto make_group = [&](uint32_t gi, RowGroup& g) {
+  auto make_group = [&](uint32_t first, uint32_t last, RowGroup& g) {
     memset(&g, 0, sizeof g);
-    const auto& gr = plan.groups[gi];
-    for (uint32_t k = gr.first; k < gr.second; k++) {
+    for (uint32_t k = first; k < last; k++) {
       if (plan.mats[k].w == 0) continue;
       g.segs[g.n_segs].ptr = leaves[k];
       g.segs[g.n_segs].width = plan.mats[k].w;
@@ -560,7 +591,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     }
   };
   // Width-0 matrices have no LDE work and are left out of the launches.
-  auto lde_group = [&](uint32_t first, uint32_t last) -> pico_status {
+  auto lde_mats = [&](uint32_t first, uint32_t last) -> pico_status {
     if (!plan.extend) return PICO_OK;
     std::vector<LdeMat> mats;
     for (uint32_t k = first; k < last; k++)
@@ -575,27 +606,52 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     return cuda_status(launch_lde(field, mats.data(), (uint32_t)mats.size(), tw, st, &c->stats.launches),
                        "LDE launch");
   };
-  c->group_ev.assign(4 * G, nullptr);
-  for (auto& e : c->group_ev)
-    if ((s = cuda_status(cudaEventCreate(&e), "event"))) {
-      destroy_events();
-      return s;
+  auto begin_phase = [&](int kind) -> pico_status {
+    pico_commit::Phase ph;
+    ph.kind = kind;
+    pico_status r;
+    if ((r = cuda_status(cudaEventCreate(&ph.begin), "event"))) return r;
+    if ((r = cuda_status(cudaEventCreate(&ph.end), "event"))) {
+      cudaEventDestroy(ph.begin);
+      return r;
     }
+    c->phases.push_back(ph);
+    return cuda_status(cudaEventRecord(ph.begin, st), "event");
+  };
+  auto end_phase = [&]() { return cuda_status(cudaEventRecord(c->phases.back().end, st), "event"); };
   uint32_t* layer = c->layers;
-  for (uint32_t gi = G; gi-- > 0;) {
-    cudaEvent_t* ge = &c->group_ev[4 * gi];
-    if (copy_in && (s = cuda_status(cudaStreamWaitEvent(st, arrived[gi], 0), "wait for inputs"))) break;
-    if ((s = cuda_status(cudaEventRecord(ge[0], st), "event"))) break;
-    if ((s = lde_group(plan.groups[gi].first, plan.groups[gi].second))) break;
-    if ((s = cuda_status(cudaEventRecord(ge[1], st), "event"))) break;
-    RowGroup g;
-    make_group(gi, g);
-    if ((s = cuda_status(cudaEventRecord(ge[2], st), "event"))) break;
-    s = cuda_status(launch_hash_rows(field, g, 1ull << plan.mats[plan.groups[gi].first].log_N,
-                                     gi == 0 ? layer : inj[gi], st),
-                    gi == 0 ? "leaf hashing" : "row hashing");
-    c->stats.launches += 1;
-    if (s || (s = cuda_status(cudaEventRecord(ge[3], st), "event"))) break;
+  for (uint32_t gi = G; gi-- > 0 && !s;) {
+    const uint32_t first = plan.groups[gi].first, last = plan.groups[gi].second;
+    const uint64_t rows = 1ull << plan.mats[first].log_N;
+    uint32_t* digests = gi == 0 ? layer : inj[gi];
+    const int hash_kind = gi == 0 ? pico_commit::kLeaves : pico_commit::kRows;
+    if (!chained[gi]) {
+      if (copy_in && (s = cuda_status(cudaStreamWaitEvent(st, arrived[last - 1], 0), "wait for inputs"))) break;
+      if ((s = begin_phase(pico_commit::kLde)) || (s = lde_mats(first, last)) || (s = end_phase())) break;
+      RowGroup g;
+      make_group(first, last, g);
+      if ((s = begin_phase(hash_kind))) break;
+      s = cuda_status(launch_hash_rows(field, g, rows, digests, st), gi == 0 ? "leaf hashing" : "row hashing");
+      c->stats.launches += 1;
+      if (s || (s = end_phase())) break;
+      continue;
+    }
+    uint32_t cols = 0, left = nonzero(gi);
+    for (uint32_t k = first; k < last && !s; k++) {
+      if (plan.mats[k].w == 0) continue;
+      left--;
+      if ((s = cuda_status(cudaStreamWaitEvent(st, arrived[k], 0), "wait for inputs"))) break;
+      if ((s = begin_phase(pico_commit::kLde)) || (s = lde_mats(k, k + 1)) || (s = end_phase())) break;
+      RowGroup g;
+      make_group(k, k + 1, g);
+      if ((s = begin_phase(hash_kind))) break;
+      s = cuda_status(launch_absorb_rows(field, g, rows, cols % 8, cols ? state : nullptr, left ? state : nullptr,
+                                         left ? nullptr : digests, st),
+                      gi == 0 ? "leaf hashing" : "row hashing");
+      c->stats.launches += 1;
+      if (s || (s = end_phase())) break;
+      cols += plan.mats[k].w;
+    }
   }
   destroy_events();
   if (s) return s;
@@ -618,10 +674,11 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
 
 // Fill c->stats timings from its events (blocks until the commit finished).
 // Events: 0 start (st), 3 compression starts (st), 4 root ready (st), 5
-// allocations done / copies may start (st), 6 copies done (copy stream);
-// per height group g, group_ev[4g .. 4g+3] bracket its LDE and its row
-// hashing on st.  lde_ms sums the LDE brackets, leaves_ms is the tallest
-// group's hashing, tree_ms the other groups' row digests plus compression.
+// allocations done / copies may start (st), 6 copies done (copy stream); each
+// entry of c->phases brackets an LDE, the tallest group's hashing or another
+// group's row digests on st.  lde_ms sums the LDE brackets, leaves_ms the
+// tallest group's hashing, tree_ms the other groups' row digests plus the
+// compression levels.
 pico_status finish_stats(pico_commit* c) {
   if (!c->ev[4]) return PICO_OK;
   pico_status s;
@@ -634,10 +691,9 @@ pico_status finish_stats(pico_commit* c) {
     return r;
   };
   double t_lde = 0, t_leaf = 0, t_tree = 0, t_tot = 0, t_h2d = 0;
-  const size_t G = c->group_ev.size() / 4;
-  for (size_t g = 0; g < G; g++) {
-    if ((s = span(c->group_ev[4 * g], c->group_ev[4 * g + 1], t_lde))) return s;
-    if ((s = span(c->group_ev[4 * g + 2], c->group_ev[4 * g + 3], g == 0 ? t_leaf : t_tree))) return s;
+  for (const pico_commit::Phase& ph : c->phases) {
+    double& acc = ph.kind == pico_commit::kLde ? t_lde : (ph.kind == pico_commit::kLeaves ? t_leaf : t_tree);
+    if ((s = span(ph.begin, ph.end, acc))) return s;
   }
   if ((s = span(c->ev[3], c->ev[4], t_tree))) return s;
   if ((s = span(c->ev[0], c->ev[4], t_tot))) return s;
@@ -664,10 +720,12 @@ void free_commit_buffers(pico_commit* c, cudaStream_t st) {
 void pico_commit::destroy_events() {
   for (int e = 0; e < 7; e++)
     if (ev[e]) cudaEventDestroy(ev[e]);
-  for (cudaEvent_t e : group_ev)
-    if (e) cudaEventDestroy(e);
+  for (const Phase& ph : phases) {
+    if (ph.begin) cudaEventDestroy(ph.begin);
+    if (ph.end) cudaEventDestroy(ph.end);
+  }
   for (cudaEvent_t& e : ev) e = nullptr;
-  group_ev.clear();
+  phases.clear();
 }
 
 pico_commit::~pico_commit() { destroy_events(); }

@@ -30,6 +30,11 @@ cudaError_t upload_p2_constants(int field, const uint32_t ext[8][16], const uint
                                 const uint32_t diag[16]);
 cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st);
 cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st);
+// Resumable row sponge: continue from state_in (nullptr: zero state) at rate
+// position pos0; if digest_out, finish and write 8-word digests, else store
+// the 16-word states to state_out.  Row r's state is 16 consecutive words.
+cudaError_t launch_absorb_rows(int field, const RowGroup& g, uint64_t rows, uint32_t pos0, const uint32_t* state_in,
+                               uint32_t* state_out, uint32_t* digest_out, cudaStream_t st);
 // next[i] = compress(prev[2i], prev[2i+1]); if inj_digests != null:
 // next[i] = compress(next[i], inj_digests[i]) (8 words per digest).
 cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,

@@ -98,6 +98,72 @@ __global__ void __launch_bounds__(256) k_hash_rows(const __grid_constant__ RowGr
   store_digest(out + 8 * r, s);
 }
 
+// The same sponge, resumable: absorb the group's columns into a state that a
+// previous call left in state_in (nullptr: the zero state), the first column
+// going to rate position pos0 of the current chunk (the previous call's
+// columns mod 8).  A call that is not the last stores the whole state to
+// state_out, including a partly overwritten chunk that is not yet permuted;
+// the last call permutes after its final (possibly partial) chunk, as the
+// one-pass sponge does, and writes the digest.  Absorbing a row's matrices
+// one call at a time gives the one-pass digest exactly.
+template <class F>
+__global__ void __launch_bounds__(256)
+    k_absorb_rows(const __grid_constant__ RowGroup g, uint64_t rows, uint32_t pos0, const uint32_t* state_in,
+                  uint32_t* state_out, uint32_t* digest_out) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  uint32_t s[16];
+  if (state_in) {
+    // plain loads: state_in may be state_out (each thread rereads its own row)
+    const uint4* p = reinterpret_cast<const uint4*>(state_in + 16 * r);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint4 v = p[k];
+      s[4 * k] = v.x;
+      s[4 * k + 1] = v.y;
+      s[4 * k + 2] = v.z;
+      s[4 * k + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; i++) s[i] = 0;
+  }
+  const int W = (int)g.total_width;
+  const int end = (int)pos0 + W;  // positions pos0 .. end-1 of the chunk sequence
+  uint32_t seg = 0, col = 0;
+  uint32_t segw = g.segs[0].width;
+  const uint32_t* rowp = g.segs[0].ptr + r * segw;
+  for (int base = 0; base < end; base += 8) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int c = base + j;  // chunk position; column c - pos0 of this call
+      if (c >= (int)pos0 && c < end) {
+        while (col == segw) {
+          seg++;
+          col = 0;
+          segw = g.segs[seg].width;
+          rowp = g.segs[seg].ptr + r * segw;
+        }
+        if (seg >= g.n_segs || col >= segw || r >= rows) {
+          hash_guard_trip(seg, col);
+          s[j] = 0;
+        } else {
+          s[j] = __ldg(rowp + col);
+        }
+        col++;
+      }
+    }
+    if (base + 8 <= end || digest_out) p2_permute<F>(s);
+  }
+  if (digest_out) {
+    store_digest(digest_out + 8 * r, s);
+  } else {
+    uint4* o = reinterpret_cast<uint4*>(state_out + 16 * r);
+#pragma unroll
+    for (int k = 0; k < 4; k++) o[k] = make_uint4(s[4 * k], s[4 * k + 1], s[4 * k + 2], s[4 * k + 3]);
+  }
+}
+
 // next[i] = compress(prev[2i], prev[2i+1]); where a matrix height meets this
 // level, next[i] = compress(next[i], inj[i]) with inj[i] the digest of the
 // concatenated rows i of those matrices (TruncatedPermutation, hash.rs:89-94;
@@ -160,6 +226,16 @@ cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32
     k_hash_rows<KoalaBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, out);
   else
     k_hash_rows<BabyBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_absorb_rows(int field, const RowGroup& g, uint64_t rows, uint32_t pos0, const uint32_t* state_in,
+                               uint32_t* state_out, uint32_t* digest_out, cudaStream_t st) {
+  if (rows == 0) return cudaSuccess;
+  if (field == 0)
+    k_absorb_rows<KoalaBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, pos0, state_in, state_out, digest_out);
+  else
+    k_absorb_rows<BabyBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, pos0, state_in, state_out, digest_out);
   return cudaGetLastError();
 }
 

@@ -110,9 +110,14 @@ struct pico_commit {
   uint64_t bytes_resident = 0;
   uint32_t root[8] = {0};
   // events (see finish_stats): compute-stream phases 0, 3, 4, copy stream 5..6,
-  // and four per height group around its LDE and its row hashing
+  // and a pair around each LDE and each row-hashing launch
   cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  std::vector<cudaEvent_t> group_ev;
+  enum PhaseKind { kLde = 0, kLeaves = 1, kRows = 2 };
+  struct Phase {
+    int kind = kLde;
+    cudaEvent_t begin = nullptr, end = nullptr;
+  };
+  std::vector<Phase> phases;
   void destroy_events();
   pico_commit_stats stats{};
   ~pico_commit();
