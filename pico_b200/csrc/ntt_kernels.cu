@@ -66,8 +66,12 @@ __device__ __noinline__ void guard_trip(int tag, unsigned long long offset, unsi
     g_lde_guard.thread = threadIdx.x;
   }
 }
-__device__ __forceinline__ bool in_range(const uint32_t* p, const GuardRange& r, int tag) {
-  if (p >= r.lo && p < r.hi) return true;
+// A set's N accesses p + k * step (k < N) are monotone: checking the first
+// and the last covers all of them.
+template <int N>
+__device__ __forceinline__ bool set_in_range(const uint32_t* p, uint64_t step, const GuardRange& r, int tag) {
+  const uint32_t* q = p + (N - 1) * step;
+  if (p >= r.lo && q < r.hi) return true;
   guard_trip(tag, (unsigned long long)(p - r.lo), (unsigned long long)(r.hi - r.lo));
   return false;
 }
@@ -446,8 +450,13 @@ __device__ __forceinline__ void load_set(uint32_t* v, const uint32_t* p, uint32_
   if (p) {
     p += (uint64_t)o * pos_step;
     const uint64_t step = pos_step << LOG_STRIDE;
+    if (set_in_range<(1 << R)>(p, step, s_in, kGuardLoad)) {
 #pragma unroll
-    for (int k = 0; k < (1 << R); k++) v[k] = in_range(p + k * step, s_in, kGuardLoad) ? __ldg(p + k * step) : 0u;
+      for (int k = 0; k < (1 << R); k++) v[k] = __ldg(p + k * step);
+    } else {
+#pragma unroll
+      for (int k = 0; k < (1 << R); k++) v[k] = 0u;
+    }
     if constexpr (Twist::active) {
       const uint2 aq = twist(o, line, (uint32_t)LOG_STRIDE);
       uint32_t cur = aq.x;
@@ -599,8 +608,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
             uint32_t col, sub;
             if (!line_at(T, ln, col, sub)) return;
             uint32_t* p = outb + (uint64_t)base * w + col;
+            if (set_in_range<(1 << RL)>(p, w, s_out, kGuardStore)) {
 #pragma unroll
-            for (int k = 0; k < (1 << RL); k++) if (in_range(p + (uint64_t)k * w, s_out, kGuardStore)) p[(uint64_t)k * w] = v[k];
+              for (int k = 0; k < (1 << RL); k++) p[(uint64_t)k * w] = v[k];
+            }
           });
     }
   }
@@ -635,8 +646,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_a(const __grid_constant__ L
     const uint32_t k1_0 = __brev(q) >> (32 - (LOG_L - 4));
     uint32_t* p = M.t1 + ((((uint64_t)k1_0 << log_n2) + j2) * w + col);
     const uint64_t step = ((uint64_t)w << log_n2) << (LOG_L - 4);
+    if (set_in_range<16>(p, step, s_out, kGuardStore)) {
 #pragma unroll
-    for (int kr = 0; kr < 16; kr++) if (in_range(p + kr * step, s_out, kGuardStore)) p[kr * step] = coef[rev_bits(kr, 4)];
+      for (int kr = 0; kr < 16; kr++) p[kr * step] = coef[rev_bits(kr, 4)];
+    }
   }
 }
 
@@ -688,8 +701,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_b(const __grid_constant__ L
           const uint32_t k1p_0 = __brev(base) >> (32 - LOG_L);
           uint32_t* p = t2 + ((((uint64_t)k1p_0 << log_n1) + k1) * w + col);
           const uint64_t step2 = ((uint64_t)w << log_n1) << (LOG_L - RL);
+          if (set_in_range<(1 << RL)>(p, step2, s_out, kGuardStore)) {
 #pragma unroll
-          for (int kr = 0; kr < (1 << RL); kr++) if (in_range(p + kr * step2, s_out, kGuardStore)) p[kr * step2] = v[rev_bits(kr, RL)];
+            for (int kr = 0; kr < (1 << RL); kr++) p[kr * step2] = v[rev_bits(kr, RL)];
+          }
         });
   }
 }
@@ -732,8 +747,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
     if (!line_at(T, ln, col, k1p)) return;
     const uint64_t row = ((uint64_t)(__brev(k1p) >> (32 - log_n2)) << LOG_L) + base;
     uint32_t* p = dst + row * w + col;
+    if (set_in_range<(1 << RL)>(p, w, s_out, kGuardStore)) {
 #pragma unroll
-    for (int k = 0; k < (1 << RL); k++) if (in_range(p + (uint64_t)k * w, s_out, kGuardStore)) p[(uint64_t)k * w] = v[k];
+      for (int k = 0; k < (1 << RL); k++) p[(uint64_t)k * w] = v[k];
+    }
   });
 }
 
