@@ -42,12 +42,14 @@ __global__ void k_permute(uint32_t* states, uint64_t n) {
 // Absorb row r of the concatenated group into a zeroed sponge state
 // (PaddingFreeSponge<_,16,8,8>: overwrite s[0..k) with each chunk of up to 8
 // elements, permute after each chunk; hash.rs:40-52).
-// Bounds guard of the row hashing: every read is checked against its
-// segment (index, column, row); a read outside is skipped (as zero) and the
-// first one recorded in g_hash_guard, which the entry points copy back with
-// their final synchronisation and report as an error.
+// Bounds guard of the row hashing: a read stays inside its row segment by
+// construction (rows are bounded by the launch, columns by the segment
+// widths), so the guard sits where the cursor moves to the next segment: a
+// move past the last segment is skipped (reads as zero), recorded in
+// g_hash_guard, and reported by the entry points after their final
+// synchronisation.
 __device__ GuardRecord g_hash_guard;
-__device__ __noinline__ void hash_guard_trip(unsigned long long seg, unsigned long long col) {
+__device__ __forceinline__ void hash_guard_trip(unsigned long long seg, unsigned long long col) {
   if (atomicAdd(&g_hash_guard.count, 1ull) == 0) {
     g_hash_guard.tag = kGuardRowRead;
     g_hash_guard.offset = seg;
@@ -66,14 +68,18 @@ __device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       if (base + j < W) {
-        while (col == segw) {
+        while (col == segw && seg < g.n_segs) {
           seg++;
           col = 0;
-          segw = g.segs[seg].width;
-          rowp = g.segs[seg].ptr + r * segw;
+          segw = seg < g.n_segs ? g.segs[seg].width : 0u;
+          rowp = g.segs[seg < g.n_segs ? seg : 0].ptr + r * segw;
         }
-        if (seg >= g.n_segs || col >= segw || r >= rows) { hash_guard_trip(seg, col); s[j] = 0; }
-        else s[j] = __ldg(rowp + col);
+        if (seg >= g.n_segs) {
+          hash_guard_trip(seg, col);
+          s[j] = 0;
+        } else {
+          s[j] = __ldg(rowp + col);
+        }
         col++;
       }
     }
@@ -88,7 +94,8 @@ __device__ __forceinline__ void store_digest(uint32_t* out, const uint32_t s[16]
 }
 
 template <class F>
-__global__ void __launch_bounds__(256) k_hash_rows(const __grid_constant__ RowGroup g, uint64_t rows, uint32_t* out) {
+// (256, 8): full occupancy at 32 registers, which the row loop fits without spills
+__global__ void __launch_bounds__(256, 8) k_hash_rows(const __grid_constant__ RowGroup g, uint64_t rows, uint32_t* out) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
   uint32_t s[16];
@@ -107,7 +114,7 @@ __global__ void __launch_bounds__(256) k_hash_rows(const __grid_constant__ RowGr
 // one-pass sponge does, and writes the digest.  Absorbing a row's matrices
 // one call at a time gives the one-pass digest exactly.
 template <class F>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 8)
     k_absorb_rows(const __grid_constant__ RowGroup g, uint64_t rows, uint32_t pos0, const uint32_t* state_in,
                   uint32_t* state_out, uint32_t* digest_out) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -138,13 +145,13 @@ __global__ void __launch_bounds__(256)
     for (int j = 0; j < 8; j++) {
       const int c = base + j;  // chunk position; column c - pos0 of this call
       if (c >= (int)pos0 && c < end) {
-        while (col == segw) {
+        while (col == segw && seg < g.n_segs) {
           seg++;
           col = 0;
-          segw = g.segs[seg].width;
-          rowp = g.segs[seg].ptr + r * segw;
+          segw = seg < g.n_segs ? g.segs[seg].width : 0u;
+          rowp = g.segs[seg < g.n_segs ? seg : 0].ptr + r * segw;
         }
-        if (seg >= g.n_segs || col >= segw || r >= rows) {
+        if (seg >= g.n_segs) {
           hash_guard_trip(seg, col);
           s[j] = 0;
         } else {
