@@ -130,6 +130,26 @@ def test_commit_uneven_batch(gpu, orc, f, b):
         pd.release()
 
 
+@pytest.mark.parametrize("f", FIELDS)
+def test_commit_chained_sponge_odd_widths(gpu, orc, f):
+    """Host inputs: a height group of many matrices is hashed matrix by matrix
+    (resumable sponge); widths 1..17 put the matrix boundaries at every rate
+    position.  Root and every layer must match the oracle, and the device-input
+    (one-pass) commit of the same matrices."""
+    shapes = [(6, w) for w in (1, 2, 3, 4, 5, 6, 7, 8, 9, 15, 17)] + [(4, 3), (4, 11), (2, 1)]
+    for plain in (False, True):
+        mats, root, pd, want_root, want_ldes, want_layers = commit_both(gpu, orc, f, shapes, 1, 700 + f, plain=plain)
+        assert root.tolist() == want_root.tolist()
+        for lvl in range(pd.log_max_height + 1):
+            got = pd.digest_layer(lvl)
+            off = sum(1 << (pd.log_max_height - l) for l in range(lvl))
+            assert (got == want_layers[off:off + got.shape[0]]).all()
+        pd.release()
+    mats, root_dev, pd, want_root, _, _ = commit_both(gpu, orc, f, shapes, 1, 700 + f, device=True)
+    assert root_dev.tolist() == want_root.tolist()
+    pd.release()
+
+
 def test_commit_device_inputs_and_rows(gpu, orc):
     f = 0
     shapes = [(12, 20), (10, 7), (12, 9)]
