@@ -264,6 +264,9 @@ def run_gpu(args, rank, world, local):
     in_bytes = 4 * cells
 
     ctx = GpuContext(local)
+    # autotune the LDE splits over the workload's heights and the hashing block size
+    heights = [lh for lh, _ in shapes]
+    tuned = ctx.autotune(field, max(12, min(heights)), max(12, max(heights))) if not args.no_tune else None
     pcs = TwoAdicFriPcs(ctx, field, b)
     doms = [TwoAdicDomain(lh) for lh, _ in shapes]
 
@@ -378,6 +381,9 @@ def run_gpu(args, rank, world, local):
             "parallelism": f"replicas x{world}",
             "l2": f"inputs ({in_bytes / 2**30:.2f} GiB) larger than L2 (126 MB); no flush"
                   if in_bytes > 126e6 else "inputs smaller than L2: not flushed",
+            "autotuned": None if tuned is None else {
+                "lde_log_n1": {str(k): v["log_n1"] for k, v in tuned.items() if k != "hash_block"},
+                "hash_block": min(tuned["hash_block"], key=tuned["hash_block"].get)},
         },
         "gpu_launches": int(sum(s["launches"] for s in stats)),
         "clocks": clocks,
@@ -619,6 +625,7 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-lde", action="store_true", help="skip the LDE-alone timing")
+    ap.add_argument("--no-tune", action="store_true", help="default LDE splits and block size (no autotuning)")
     args = ap.parse_args()
 
     rank, world, local = dist_setup(args.gpus)

@@ -219,6 +219,23 @@ pico_status pico_gpu_cancel(pico_ctx *ctx, pico_request *req);
 pico_status pico_gpu_request_times(const pico_request *req, double *queued_us, double *run_us);
 pico_status pico_gpu_request_free(pico_ctx *ctx, pico_request *req);
 
+/* ---- autotuning (no counterpart in the reference; Plonky3's CPU path has
+ * nothing to tune) -----------------------------------------------------------
+ * pico_gpu_autotune times, on this device, the candidate four-step splits
+ * n = n1 * n2 of the coset LDE for every height 2^log_n_min .. 2^log_n_max
+ * that uses the three-pass form (n > 2^11), and the row-hashing block size,
+ * and keeps the fastest in the context; later commits and LDEs of that field
+ * use them.  Results are bit-identical for every choice.  ms_out (nullable)
+ * receives 3 times per height (splits ceil(log_n/2) - 1, + 0, + 1; 0 where a
+ * split is not valid) followed by 3 times for blocks 64, 128, 256.  Call it
+ * before submitting work that should use the tuned values. */
+pico_status pico_gpu_autotune(pico_ctx *ctx, pico_field field, uint32_t log_n_min, uint32_t log_n_max,
+                              float *ms_out);
+/* Read (and if set_log_n1 != 0, first set) the split used at height 2^log_n:
+ * *log_n1_out = log2 n1, or 0 for the one-pass form. */
+pico_status pico_gpu_lde_split(pico_ctx *ctx, pico_field field, uint32_t log_n, uint32_t set_log_n1,
+                               uint32_t *log_n1_out);
+
 #ifdef __cplusplus
 }
 #endif

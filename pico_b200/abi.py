@@ -128,6 +128,8 @@ SIGNATURES = {
     "pico_gpu_cancel": (C.c_int, [_vp, _vp]),
     "pico_gpu_request_times": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "pico_gpu_request_free": (C.c_int, [_vp, _vp]),
+    "pico_gpu_autotune": (C.c_int, [_vp, C.c_int, _u32, _u32, C.POINTER(C.c_float)]),
+    "pico_gpu_lde_split": (C.c_int, [_vp, C.c_int, _u32, _u32, C.POINTER(_u32)]),
 }
 
 _lib = None

@@ -460,7 +460,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       L.w = m.w;
       L.shift = m.shift % (field == 0 ? KoalaBear::P : BabyBear::P);
       L.pw = (uint32_t*)pw + (uint64_t)k * nb * kPwWords;
-      plan_lde_tiling(L);
+      plan_lde_tiling(L, m.log_n <= kLdeMaxLogN ? ctx->lde_split[field][m.log_n] : 0u);
       void* out;
       if ((s = alloc_async(&out, ((uint64_t)m.w << m.log_N) * 4, st))) return s;
       L.out = (uint32_t*)out;
@@ -631,7 +631,8 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       RowGroup g;
       make_group(first, last, g);
       if ((s = begin_phase(hash_kind))) break;
-      s = cuda_status(launch_hash_rows(field, g, rows, digests, st), gi == 0 ? "leaf hashing" : "row hashing");
+      s = cuda_status(launch_hash_rows(field, g, rows, digests, st, ctx->hash_block[field]),
+                      gi == 0 ? "leaf hashing" : "row hashing");
       c->stats.launches += 1;
       if (s || (s = end_phase())) break;
       continue;
@@ -646,7 +647,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       make_group(k, k + 1, g);
       if ((s = begin_phase(hash_kind))) break;
       s = cuda_status(launch_absorb_rows(field, g, rows, cols % 8, cols ? state : nullptr, left ? state : nullptr,
-                                         left ? nullptr : digests, st),
+                                         left ? nullptr : digests, st, ctx->hash_block[field]),
                       gi == 0 ? "leaf hashing" : "row hashing");
       c->stats.launches += 1;
       if (s || (s = end_phase())) break;
@@ -966,7 +967,7 @@ extern "C" pico_status pico_gpu_coset_lde_batch(pico_ctx* ctx, pico_field field,
   L.log_n = log_n;
   L.log_b = log_blowup;
   L.w = width;
-  plan_lde_tiling(L);
+  plan_lde_tiling(L, ctx->lde_split[field][log_n]);
   const uint64_t in_bytes = ((uint64_t)width << log_n) * 4;
   auto run = [&]() -> pico_status {
     void* p;
@@ -1042,4 +1043,154 @@ extern "C" pico_status pico_gpu_poseidon2_permute(pico_ctx* ctx, pico_field fiel
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "permute");
   unreserve(ctx, bytes);
   return s ? s : s2;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuning
+
+extern "C" pico_status pico_gpu_lde_split(pico_ctx* ctx, pico_field field, uint32_t log_n, uint32_t set_log_n1,
+                                          uint32_t* log_n1_out) {
+  using namespace pico;
+  if (!ctx || (field != PICO_KOALABEAR && field != PICO_BABYBEAR) || log_n > kLdeMaxLogN) {
+    set_error("lde_split: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (set_log_n1) {
+    if (!lde_split_valid(log_n, set_log_n1)) {
+      set_error("lde_split: 2^%u = 2^%u x 2^%u is not a valid split (factors 2^6 .. 2^12, n > 2^11)", log_n,
+                set_log_n1, log_n - set_log_n1);
+      return PICO_ERR_INVALID_ARG;
+    }
+    ctx->lde_split[field][log_n] = (uint8_t)set_log_n1;
+  }
+  if (log_n1_out) {
+    LdeMat m;
+    memset(&m, 0, sizeof m);
+    m.log_n = log_n;
+    plan_lde_tiling(m, ctx->lde_split[field][log_n]);
+    *log_n1_out = m.log_n1;
+  }
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_autotune(pico_ctx* ctx, pico_field field, uint32_t log_n_min, uint32_t log_n_max,
+                                         float* ms_out) {
+  using namespace pico;
+  if (!ctx || (field != PICO_KOALABEAR && field != PICO_BABYBEAR) || log_n_min > log_n_max) {
+    set_error("autotune: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint32_t lo = std::max<uint32_t>(log_n_min, kLdeSmallMaxLog + 1);
+  const uint32_t hi = std::min<uint32_t>(log_n_max, std::min<uint32_t>(kLdeMaxLogN, field_two_adicity(field) - 1));
+  cudaSetDevice(ctx->device);
+  uint32_t slot = 0;
+  cudaStream_t st = pick_stream(ctx, nullptr, &slot);
+  // Synthetic inputs of 2^26 words at most (w = 2^26 / n columns, 4 .. 64),
+  // log_blowup 1; the values are zero (timing does not depend on them).
+  auto width_for = [](uint32_t log_n) { return std::min<uint32_t>(64, std::max<uint32_t>(4, 1u << (26 - std::min(log_n, 26u)))); };
+  uint64_t in_words = 1u << 20, out_words = 2u << 20;
+  for (uint32_t l = lo; l <= hi; l++) {
+    in_words = std::max<uint64_t>(in_words, (uint64_t)width_for(l) << l);
+    out_words = std::max<uint64_t>(out_words, (uint64_t)width_for(l) << (l + 1));
+  }
+  const uint64_t hash_rows = 1u << 20, hash_w = 64;
+  out_words = std::max<uint64_t>(out_words, hash_rows * hash_w);
+  const uint64_t need = (2 * in_words + 2 * out_words + 2 * kPwWords + hash_rows * 8) * 4;
+  if (!try_reserve(ctx, need)) {
+    set_error("autotune: HBM budget exceeded");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  std::vector<void*> bufs;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const TwiddleTables tw = twiddles(ctx, field);
+  auto run = [&]() -> pico_status {
+    pico_status s;
+    void *in, *out, *t1, *t2, *pw, *dig;
+    if ((s = alloc_async(&in, in_words * 4, st)) || (s = alloc_async(&out, out_words * 4, st)) ||
+        (s = alloc_async(&t1, in_words * 4, st)) || (s = alloc_async(&t2, out_words * 4, st)) ||
+        (s = alloc_async(&pw, 2 * kPwWords * 4, st)) || (s = alloc_async(&dig, hash_rows * 32, st)))
+      return s;
+    bufs = {in, out, t1, t2, pw, dig};
+    if ((s = cuda_status(cudaMemsetAsync(in, 0, in_words * 4, st), "memset")) ||
+        (s = cuda_status(cudaMemsetAsync(out, 0, out_words * 4, st), "memset")) ||
+        (s = cuda_status(cudaEventCreate(&e0), "event")) || (s = cuda_status(cudaEventCreate(&e1), "event")))
+      return s;
+    // time fn over 3 launches after one warm-up; ms per launch
+    auto timeit = [&](auto fn, float& ms) -> pico_status {
+      pico_status r;
+      if ((r = fn())) return r;
+      if ((r = cuda_status(cudaEventRecord(e0, st), "event"))) return r;
+      for (int i = 0; i < 3; i++)
+        if ((r = fn())) return r;
+      if ((r = cuda_status(cudaEventRecord(e1, st), "event")) ||
+          (r = cuda_status(cudaEventSynchronize(e1), "autotune")) ||
+          (r = cuda_status(cudaEventElapsedTime(&ms, e0, e1), "event timing")))
+        return r;
+      ms /= 3;
+      return PICO_OK;
+    };
+    for (uint32_t l = lo; l <= hi; l++) {
+      const uint32_t def = (l + 1) / 2;
+      float best = 0;
+      uint32_t best_n1 = 0;
+      for (int c = 0; c < 3; c++) {
+        const uint32_t n1 = def - 1 + c;
+        float ms = 0;
+        if (lde_split_valid(l, n1)) {
+          LdeMat m;
+          memset(&m, 0, sizeof m);
+          m.in = (const uint32_t*)in;
+          m.out = (uint32_t*)out;
+          m.t1 = (uint32_t*)t1;
+          m.t2 = (uint32_t*)t2;
+          m.pw = (uint32_t*)pw;
+          m.log_n = l;
+          m.log_b = 1;
+          m.w = width_for(l);
+          m.shift = field == 0 ? KoalaBear::ONE : BabyBear::ONE;
+          plan_lde_tiling(m, n1);
+          if ((s = timeit([&]() { return cuda_status(launch_lde(field, &m, 1, tw, st), "LDE"); }, ms))) return s;
+          if (!best_n1 || ms < best) {
+            best = ms;
+            best_n1 = n1;
+          }
+        }
+        if (ms_out) ms_out[3 * (l - log_n_min) + c] = ms;
+      }
+      if (best_n1) ctx->lde_split[field][l] = (uint8_t)best_n1;
+    }
+    RowGroup g;
+    memset(&g, 0, sizeof g);
+    g.n_segs = 1;
+    g.segs[0].ptr = (const uint32_t*)out;
+    g.segs[0].width = (uint32_t)hash_w;
+    g.total_width = (uint32_t)hash_w;
+    float best = 0;
+    uint32_t best_block = 256;
+    for (int c = 0; c < 3; c++) {
+      const unsigned block = 64u << c;
+      float ms = 0;
+      if ((s = timeit([&]() {
+             return cuda_status(launch_hash_rows(field, g, hash_rows, (uint32_t*)dig, st, block), "hash rows");
+           }, ms)))
+        return s;
+      if (c == 0 || ms < best) {
+        best = ms;
+        best_block = block;
+      }
+      if (ms_out) ms_out[3 * (log_n_max - log_n_min + 1) + c] = ms;
+    }
+    ctx->hash_block[field] = best_block;
+    return PICO_OK;
+  };
+  pico_status s = run();
+  for (void* p : bufs) cudaFreeAsync(p, st);
+  if (!s) s = guard_enqueue(ctx, slot, st);
+  pico_status s2 = cuda_status(cudaStreamSynchronize(st), "autotune");
+  if (!s) s = s2;
+  if (!s) s = guard_verdict(ctx, slot);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  unreserve(ctx, need);
+  return s;
 }

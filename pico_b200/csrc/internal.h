@@ -29,12 +29,13 @@ struct RowGroup {
 cudaError_t upload_p2_constants(int field, const uint32_t ext[8][16], const uint32_t* inte, int rounds_p,
                                 const uint32_t diag[16]);
 cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st);
-cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st);
+cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st,
+                             unsigned block = 256);
 // Resumable row sponge: continue from state_in (nullptr: zero state) at rate
 // position pos0; if digest_out, finish and write 8-word digests, else store
 // the 16-word states to state_out.  Row r's state is 16 consecutive words.
 cudaError_t launch_absorb_rows(int field, const RowGroup& g, uint64_t rows, uint32_t pos0, const uint32_t* state_in,
-                               uint32_t* state_out, uint32_t* digest_out, cudaStream_t st);
+                               uint32_t* state_out, uint32_t* digest_out, cudaStream_t st, unsigned block = 256);
 // next[i] = compress(prev[2i], prev[2i+1]); if inj_digests != null:
 // next[i] = compress(next[i], inj_digests[i]) (8 words per digest).
 cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,
@@ -122,6 +123,10 @@ cudaError_t launch_lde(int field, const LdeMat* mats, uint32_t n, TwiddleTables 
                        uint64_t* launches = nullptr);
 
 // Choose the one-pass or three-pass form for one matrix (fills log_n1, log_n2).
-void plan_lde_tiling(LdeMat& m);
+// One-pass form for n <= 2^11; above, the four-step split n = n1 * n2 with
+// log_n1 if it is a valid split (both factors 2^6 .. 2^12), else the default
+// n1 = 2^ceil(log_n / 2).
+void plan_lde_tiling(LdeMat& m, uint32_t log_n1 = 0);
+bool lde_split_valid(uint32_t log_n, uint32_t log_n1);
 
 }  // namespace pico

@@ -778,9 +778,17 @@ __global__ void k_pow_tables(const __grid_constant__ LdeBatch batch, const __gri
   M.pw[i] = v;
 }
 
-void plan_lde_tiling(LdeMat& m) {
+bool lde_split_valid(uint32_t log_n, uint32_t log_n1) {
+  return log_n > (uint32_t)kLdeSmallMaxLog && log_n <= kLdeMaxLogN && log_n1 >= (uint32_t)kMinLogL3 &&
+         log_n1 <= (uint32_t)kMaxLogL && log_n - log_n1 >= (uint32_t)kMinLogL3 && log_n - log_n1 <= (uint32_t)kMaxLogL;
+}
+
+void plan_lde_tiling(LdeMat& m, uint32_t log_n1) {
   if ((int)m.log_n <= kLdeSmallMaxLog) {
     m.log_n1 = m.log_n2 = 0;
+  } else if (lde_split_valid(m.log_n, log_n1)) {
+    m.log_n1 = log_n1;
+    m.log_n2 = m.log_n - log_n1;
   } else {
     m.log_n1 = (m.log_n + 1) / 2;
     m.log_n2 = m.log_n / 2;

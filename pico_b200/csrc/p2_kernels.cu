@@ -227,22 +227,28 @@ cudaError_t hash_guard_clear() {
   return cudaMemcpyToSymbol(g_hash_guard, &z, sizeof z);
 }
 
-cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st) {
+// block: threads per CTA, 32 .. 256 (the kernels are bounded to 256).
+cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st,
+                             unsigned block) {
   if (rows == 0) return cudaSuccess;
+  if (block < 32 || block > 256) block = 256;
   if (field == 0)
-    k_hash_rows<KoalaBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, out);
+    k_hash_rows<KoalaBear><<<blocks_for(rows, block), block, 0, st>>>(g, rows, out);
   else
-    k_hash_rows<BabyBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, out);
+    k_hash_rows<BabyBear><<<blocks_for(rows, block), block, 0, st>>>(g, rows, out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_absorb_rows(int field, const RowGroup& g, uint64_t rows, uint32_t pos0, const uint32_t* state_in,
-                               uint32_t* state_out, uint32_t* digest_out, cudaStream_t st) {
+                               uint32_t* state_out, uint32_t* digest_out, cudaStream_t st, unsigned block) {
   if (rows == 0) return cudaSuccess;
+  if (block < 32 || block > 256) block = 256;
   if (field == 0)
-    k_absorb_rows<KoalaBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, pos0, state_in, state_out, digest_out);
+    k_absorb_rows<KoalaBear><<<blocks_for(rows, block), block, 0, st>>>(g, rows, pos0, state_in, state_out,
+                                                                        digest_out);
   else
-    k_absorb_rows<BabyBear><<<blocks_for(rows, 256), 256, 0, st>>>(g, rows, pos0, state_in, state_out, digest_out);
+    k_absorb_rows<BabyBear><<<blocks_for(rows, block), block, 0, st>>>(g, rows, pos0, state_in, state_out,
+                                                                       digest_out);
   return cudaGetLastError();
 }
 

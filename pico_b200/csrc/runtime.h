@@ -93,6 +93,10 @@ struct pico_ctx {
   pico::GuardRecord* guard_host = nullptr;  // pinned: 2 records (LDE, hashing) per stream slot
   pico::Server* server = nullptr;
   uint32_t max_inflight = 0;  // serving: requests on the device at once
+  // Autotuned choices (pico_gpu_autotune), per field: the LDE's four-step
+  // split log2 n1 per height (0 = default) and the row-hashing block size.
+  uint8_t lde_split[2][pico::kLdeMaxLogN + 1] = {};
+  uint32_t hash_block[2] = {256, 256};
   ~pico_ctx();
 };
 

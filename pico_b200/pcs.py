@@ -70,6 +70,28 @@ class GpuContext:
         abi.check(self.lib.pico_gpu_memory(self.handle, C.byref(r), C.byref(b)))
         return r.value, b.value
 
+    def autotune(self, field, log_n_min: int = 12, log_n_max: int = 22) -> dict:
+        """Time the LDE's four-step splits per height and the row-hashing block
+        size on this device and keep the fastest (pico_gpu_autotune).  Returns
+        {log_n: {"log_n1": chosen, "ms": {log_n1: ms}}, "hash_block": {block: ms}}."""
+        f = F.field_id(field)
+        heights = log_n_max - log_n_min + 1
+        ms = (C.c_float * (3 * heights + 3))()
+        abi.check(self.lib.pico_gpu_autotune(self.handle, f, log_n_min, log_n_max, ms))
+        out = {}
+        for i, l in enumerate(range(log_n_min, log_n_max + 1)):
+            times = {(l + 1) // 2 - 1 + c: ms[3 * i + c] for c in range(3) if ms[3 * i + c] > 0}
+            if times:
+                out[l] = {"log_n1": self.lde_split(f, l), "ms": times}
+        out["hash_block"] = {64 << c: ms[3 * heights + c] for c in range(3)}
+        return out
+
+    def lde_split(self, field, log_n: int, set_log_n1: int = 0) -> int:
+        """log2 n1 of the LDE's four-step split at height 2^log_n (0: one pass); set it if set_log_n1."""
+        v = C.c_uint32()
+        abi.check(self.lib.pico_gpu_lde_split(self.handle, F.field_id(field), log_n, set_log_n1, C.byref(v)))
+        return v.value
+
 
 @dataclass
 class TwoAdicDomain:

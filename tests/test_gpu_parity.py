@@ -131,6 +131,40 @@ def test_commit_uneven_batch(gpu, orc, f, b):
 
 
 @pytest.mark.parametrize("f", FIELDS)
+def test_lde_every_split_bit_exact(gpu, orc, f):
+    """Every four-step split the autotuner may choose gives the same LDE."""
+    for logn, w in ((12, 5), (13, 3), (14, 9)):
+        m = F.random_matrix(f, logn, w, 40 + logn)
+        want = orc.coset_lde(f, m, 1, F.lde_shift(f))
+        default = gpu.lde_split(f, logn)
+        try:
+            for n1 in range(6, 13):
+                if not 6 <= logn - n1 <= 12:
+                    with pytest.raises(PicoError):
+                        gpu.lde_split(f, logn, n1)
+                    continue
+                assert gpu.lde_split(f, logn, n1) == n1
+                got = Radix2DitParallel(gpu, f).coset_lde_batch_bitrev(m, 1, F.lde_shift(f))
+                assert (got == want).all(), (logn, n1)
+        finally:
+            gpu.lde_split(f, logn, default)
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_autotune_keeps_parity(gpu, orc, f):
+    rep = gpu.autotune(f, 12, 15)
+    assert set(rep) >= {12, 13, 14, 15, "hash_block"}
+    for l in range(12, 16):
+        assert rep[l]["log_n1"] in rep[l]["ms"]
+    shapes = [(15, 7), (13, 20), (12, 3), (9, 11)]
+    mats, root, pd, want_root, want_ldes, _ = commit_both(gpu, orc, f, shapes, 1, 800 + f)
+    assert root.tolist() == want_root.tolist()
+    for i in range(len(mats)):
+        assert (pd.lde(i) == want_ldes[i]).all()
+    pd.release()
+
+
+@pytest.mark.parametrize("f", FIELDS)
 def test_commit_chained_sponge_odd_widths(gpu, orc, f):
     """Host inputs: a height group of many matrices is hashed matrix by matrix
     (resumable sponge); widths 1..17 put the matrix boundaries at every rate
