@@ -53,7 +53,7 @@ typedef enum { PICO_KOALABEAR = 0, PICO_BABYBEAR = 1 } pico_field;
 
 /* Flags for commit / LDE / FRI calls. */
 #define PICO_INPUT_DEVICE 0x1u /* input pointers are device pointers (else host) */
-#define PICO_COMMIT_PLAIN 0x2u /* one matrix per launch, no graph: the baseline form */
+#define PICO_COMMIT_PLAIN 0x2u /* one matrix per launch (LDE and row hashing): the baseline form */
 #define PICO_OUTPUT_DEVICE 0x4u /* output pointers are device pointers (else host) */
 #define PICO_LDE_NATURAL_ORDER 0x8u /* coset_lde_batch: natural row order (Dft trait); default bit-reversed */
 

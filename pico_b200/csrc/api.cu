@@ -374,7 +374,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
     }
     const uint64_t rows = 1ull << plan.mats[plan.groups[gi].first].log_N;
     if (gi > 0) scr += rows * 32;  // injected-row digests
-    if (!plan.input_device && nonzero >= 2) state_rows = std::max(state_rows, rows);
+    if ((!plan.input_device || plan.plain) && nonzero >= 2) state_rows = std::max(state_rows, rows);
     const uint64_t absorb = rows * ((wsum + 7) / 8);
     if (gi == 0)
       plan.leaf_permutations = absorb;
@@ -511,6 +511,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   // With host inputs, a group of several matrices is hashed one matrix at a
   // time as each arrives (resumable sponge), the row states kept in `state`
   // between matrices; its size is the largest such group's rows x 16 words.
+  // The plain form hashes matrix by matrix too (one launch per matrix).
   auto nonzero = [&](uint32_t gi) {
     uint32_t c = 0;
     for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) c += plan.mats[k].w != 0;
@@ -521,7 +522,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   {
     uint64_t rows_max = 0;
     for (uint32_t gi = 0; gi < G; gi++) {
-      chained[gi] = copy_in && nonzero(gi) >= 2;
+      chained[gi] = (copy_in || plan.plain) && nonzero(gi) >= 2;
       if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
     }
     if (rows_max) {
@@ -641,7 +642,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     for (uint32_t k = first; k < last && !s; k++) {
       if (plan.mats[k].w == 0) continue;
       left--;
-      if ((s = cuda_status(cudaStreamWaitEvent(st, arrived[k], 0), "wait for inputs"))) break;
+      if (copy_in && (s = cuda_status(cudaStreamWaitEvent(st, arrived[k], 0), "wait for inputs"))) break;
       if ((s = begin_phase(pico_commit::kLde)) || (s = lde_mats(k, k + 1)) || (s = end_phase())) break;
       RowGroup g;
       make_group(k, k + 1, g);
