@@ -29,6 +29,19 @@ class Challenger(C.Structure):
     ]
 
 
+class OpenBatch(C.Structure):
+    _fields_ = [
+        ("n_mats", C.c_uint32),
+        ("ldes", C.c_void_p),
+        ("log_heights", C.c_void_p),
+        ("widths", C.c_void_p),
+        ("n_points", C.c_void_p),
+        ("points", C.c_void_p),
+        ("layers", C.c_void_p),
+        ("root", C.c_void_p),
+    ]
+
+
 def build(force: bool = False) -> Path:
     srcs = [HERE / "oracle.c", HERE / "oracle.h", HERE.parent / "pico_b200" / "csrc" / "p2_rc_table.inc"]
     if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
@@ -64,6 +77,16 @@ def load():
                 ("orc_fri_commit_phase", C.c_int,
                  [C.c_int, vp, u32, u32, u32, vp, C.POINTER(Challenger), vp, vp, vp, vp]),
                 ("orc_ext_mul", None, [C.c_int, vp, vp, vp]),
+                ("orc_ext_inv", None, [C.c_int, vp, vp]),
+                ("orc_open_values", C.c_int, [C.c_int, C.POINTER(OpenBatch), u32, vp]),
+                ("orc_reduce_openings", C.c_int, [C.c_int, C.POINTER(OpenBatch), u32, vp, vp, u32, vp]),
+                ("orc_open_query_words", u64, [C.POINTER(OpenBatch), u32, u32]),
+                ("orc_pcs_open", C.c_int,
+                 [C.c_int, C.POINTER(OpenBatch), u32, u32, u32, u32, C.POINTER(Challenger), vp, vp, vp, vp, vp,
+                  vp, vp, vp]),
+                ("orc_verify_open", C.c_int,
+                 [C.c_int, C.POINTER(OpenBatch), u32, u32, u32, u32, C.POINTER(Challenger), vp, vp, u32, vp, u32,
+                  vp, vp]),
             ]:
                 fn = getattr(lib, name)
                 fn.restype = res
@@ -199,3 +222,106 @@ def ext_mul(field: int, a, b) -> np.ndarray:
     out = np.zeros(4, dtype=np.uint32)
     load().orc_ext_mul(field, x.ctypes.data, y.ctypes.data, out.ctypes.data)
     return out
+
+
+def ext_inv(field: int, a) -> np.ndarray:
+    x = _u32(a)
+    out = np.zeros(4, dtype=np.uint32)
+    load().orc_ext_inv(field, x.ctypes.data, out.ctypes.data)
+    return out
+
+
+class _Batches:
+    """ctypes view of opening batches.  Each batch is a dict with `ldes`
+    (committed LDEs, bit-reversed rows, Monty), `points` (per matrix an array
+    of shape (k, 4)), and optionally `layers` and `root`."""
+
+    def __init__(self, batches):
+        self.keep = []
+        arr = (OpenBatch * len(batches))()
+        for b, B in enumerate(batches):
+            ldes = [_u32(m) for m in B["ldes"]]
+            n = len(ldes)
+            ptrs = (C.c_void_p * n)(*[m.ctypes.data for m in ldes])
+            logh = np.array([m.shape[0].bit_length() - 1 for m in ldes], dtype=np.uint32)
+            widths = np.array([m.shape[1] for m in ldes], dtype=np.uint32)
+            pts = [np.asarray(P, dtype=np.uint32).reshape(-1, 4) for P in B["points"]]
+            npts = np.array([len(P) for P in pts], dtype=np.uint32)
+            flat = _u32(np.concatenate(pts) if sum(len(P) for P in pts) else np.zeros((1, 4), np.uint32))
+            layers = _u32(B["layers"]) if B.get("layers") is not None else None
+            root = _u32(B["root"]) if B.get("root") is not None else None
+            self.keep += [ldes, ptrs, logh, widths, npts, flat, layers, root]
+            arr[b] = OpenBatch(n, C.cast(ptrs, C.c_void_p), logh.ctypes.data, widths.ctypes.data,
+                               npts.ctypes.data, flat.ctypes.data,
+                               layers.ctypes.data if layers is not None else None,
+                               root.ctypes.data if root is not None else None)
+        self.arr = arr
+        self.n = len(batches)
+        self.value_words = sum(4 * len(P) * m.shape[1] for B in batches for m, P in zip(B["ldes"], B["points"])
+                               if len(np.asarray(P)))
+
+
+def open_values(field: int, batch, log_blowup: int) -> np.ndarray:
+    bs = _Batches([batch])
+    out = np.zeros(max(bs.value_words, 4), dtype=np.uint32)
+    _check(load().orc_open_values(field, bs.arr, log_blowup, out.ctypes.data), "open_values")
+    return out[: bs.value_words].reshape(-1, 4)
+
+
+def reduce_openings(field: int, batches, values, alpha, log_height: int) -> np.ndarray:
+    bs = _Batches(batches)
+    v = _u32(values)
+    a = _u32(alpha)
+    out = np.zeros((1 << log_height, 4), dtype=np.uint32)
+    _check(load().orc_reduce_openings(field, bs.arr, bs.n, v.ctypes.data, a.ctypes.data, log_height,
+                                      out.ctypes.data), "reduce_openings")
+    return out
+
+
+def open_query_words(batches, log_blowup: int) -> int:
+    return int(load().orc_open_query_words(_Batches(batches).arr, len(batches), log_blowup))
+
+
+def pcs_open(field: int, batches, log_blowup: int, num_queries: int, pow_bits: int, challenger=None):
+    """TwoAdicFriPcs::open; returns a dict of the opened values and the proof."""
+    bs = _Batches(batches)
+    log_max = max(m.shape[0].bit_length() - 1 for B in batches for m in B["ldes"])
+    rounds = log_max - log_blowup
+    qw = int(load().orc_open_query_words(bs.arr, bs.n, log_blowup))
+    values = np.zeros(max(bs.value_words, 4), dtype=np.uint32)
+    roots = np.zeros((max(rounds, 1), 8), dtype=np.uint32)
+    betas = np.zeros((max(rounds, 1), 4), dtype=np.uint32)
+    final = np.zeros(4, dtype=np.uint32)
+    wit = C.c_uint32()
+    idx = np.zeros(max(num_queries, 1), dtype=np.uint32)
+    queries = np.zeros((max(num_queries, 1), qw), dtype=np.uint32)
+    nr = C.c_uint32()
+    ch = challenger if challenger is not None else new_challenger()
+    _check(load().orc_pcs_open(field, bs.arr, bs.n, log_blowup, num_queries, pow_bits, C.byref(ch),
+                               values.ctypes.data, roots.ctypes.data, betas.ctypes.data, final.ctypes.data,
+                               C.byref(wit), idx.ctypes.data, queries.ctypes.data, C.byref(nr)), "pcs_open")
+    return {
+        "values": values[: bs.value_words].reshape(-1, 4),
+        "roots": roots[:rounds],
+        "betas": betas[:rounds],
+        "final": final,
+        "pow_witness": int(wit.value),
+        "indices": idx[:num_queries],
+        "queries": queries[:num_queries],
+        "challenger": ch,
+    }
+
+
+def verify_open(field: int, batches, log_blowup: int, num_queries: int, pow_bits: int, proof, challenger=None):
+    """The Pico verifier's checks; returns (code, indices), code 0 = verifies."""
+    bs = _Batches(batches)
+    ch = challenger if challenger is not None else new_challenger()
+    v = _u32(proof["values"])
+    roots = _u32(proof["roots"])
+    fin = _u32(proof["final"])
+    q = _u32(proof["queries"])
+    idx = np.zeros(max(num_queries, 1), dtype=np.uint32)
+    rc = load().orc_verify_open(field, bs.arr, bs.n, log_blowup, num_queries, pow_bits, C.byref(ch),
+                                v.ctypes.data, roots.ctypes.data, len(proof["roots"]), fin.ctypes.data,
+                                int(proof["pow_witness"]), q.ctypes.data, idx.ctypes.data)
+    return rc, idx[:num_queries]

@@ -628,3 +628,609 @@ int orc_fri_commit_phase(int field, const uint32_t *codeword, uint32_t log_n,
     free(nxt);
     return ORC_OK;
 }
+
+/* ===================== PCS opening (TwoAdicFriPcs::open) =====================
+ * The prover side of the opening, restated from what the Pico verifier checks
+ * (every step below is fixed by vm/src/compiler/recursion/circuit/fri.rs):
+ *   - every opened value is observed (its 4 base coefficients, in batch /
+ *     matrix / point / column order) before alpha is sampled: fri.rs:85-99;
+ *   - reduced openings per LDE height, with the powers of alpha counted per
+ *     height in that same order and x = g * w_h^rev(index): fri.rs:113-238;
+ *   - the FRI commit phase folds the tallest reduced opening and adds each
+ *     shorter one once the folded length reaches its height: fri.rs:300-318;
+ *   - the final polynomial is observed, the proof-of-work witness checked and
+ *     the query indices sampled: fri.rs:54-70 (check_witness / sample_bits:
+ *     challenger.rs:109-115, 210-221);
+ *   - query openings: an MMCS batch opening of every input batch
+ *     (fri.rs:389-436) and the commit-phase sibling values and paths
+ *     (fri.rs:320-343).
+ * Opened values follow Plonky3's interpolate_coset: barycentric evaluation
+ * over the low coset g * H_n held in the first n rows of each committed LDE.
+ */
+
+static void ext_add_c(uint32_t p, const uint32_t *a, const uint32_t *b, uint32_t *o) {
+    for (int i = 0; i < 4; i++) o[i] = fadd(p, a[i], b[i]);
+}
+static void ext_sub_c(uint32_t p, const uint32_t *a, const uint32_t *b, uint32_t *o) {
+    for (int i = 0; i < 4; i++) o[i] = fsub(p, a[i], b[i]);
+}
+static void ext_scale_c(uint32_t p, const uint32_t *a, uint32_t s, uint32_t *o) {
+    for (int i = 0; i < 4; i++) o[i] = fmul(p, a[i], s);
+}
+static void ext_pow_c(const field_t *F, const uint32_t *a, uint64_t e, uint32_t *o) {
+    uint32_t r[4] = {1, 0, 0, 0}, b[4];
+    memcpy(b, a, 16);
+    while (e) {
+        if (e & 1) ext_mul_c(F->p, F->w_ext, r, b, r);
+        ext_mul_c(F->p, F->w_ext, b, b, b);
+        e >>= 1;
+    }
+    memcpy(o, r, 16);
+}
+/* Inverse through the norm to F_p: a^-1 = a^p a^(p^2) a^(p^3) / N(a).  With
+ * X^4 = W the Frobenius maps X to gamma X, gamma = W^((p-1)/4), so the k-th
+ * conjugate multiplies coefficient i by gamma^(k i). */
+static void ext_inv_c(const field_t *F, const uint32_t *a, uint32_t *o) {
+    uint32_t p = F->p;
+    uint32_t gamma = fpow(p, F->w_ext, (p - 1) / 4);
+    uint32_t c1[4], c2[4], c3[4], t[4], n[4];
+    for (int i = 0; i < 4; i++) {
+        c1[i] = fmul(p, a[i], fpow(p, gamma, (uint64_t)i));
+        c2[i] = fmul(p, a[i], fpow(p, gamma, 2ull * i));
+        c3[i] = fmul(p, a[i], fpow(p, gamma, 3ull * i));
+    }
+    ext_mul_c(p, F->w_ext, c1, c2, t);
+    ext_mul_c(p, F->w_ext, t, c3, t);
+    ext_mul_c(p, F->w_ext, a, t, n); /* n[1..3] == 0 */
+    ext_scale_c(p, t, finv(p, n[0]), o);
+}
+
+void orc_ext_inv(int field, const uint32_t a[4], uint32_t out[4]) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    uint32_t x[4], y[4];
+    for (int i = 0; i < 4; i++) x[i] = c_from(c, a[i]);
+    ext_inv_c(F, x, y);
+    for (int i = 0; i < 4; i++) out[i] = c_to(c, y[i]);
+}
+
+/* g * w_h^rev_h(i), canonical. */
+static uint32_t lde_point(const field_t *F, uint32_t wh, uint32_t log_h, uint64_t i) {
+    return fmul(F->p, F->generator, fpow(F->p, wh, bitrev(i, log_h)));
+}
+
+/* p(z) for every column of one matrix (interpolate_coset); z and out canonical. */
+static int open_one(const field_t *F, conv_t c, int field, const uint32_t *lde, uint32_t log_N, uint32_t w,
+                    uint32_t log_b, const uint32_t *z, uint32_t *out) {
+    uint32_t p = F->p;
+    uint32_t log_n = log_N - log_b;
+    uint64_t n = 1ull << log_n;
+    uint32_t *coef = malloc(n * 16);
+    if (!coef) return ORC_ENOMEM;
+    uint32_t wn = orc_two_adic_generator(field, log_n);
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < (long long)n; k++) {
+        uint32_t wk = fpow(p, wn, (uint64_t)k);
+        uint32_t d[4];
+        memcpy(d, z, 16);
+        d[0] = fsub(p, d[0], fmul(p, F->generator, wk));
+        uint32_t di[4];
+        ext_inv_c(F, d, di);
+        ext_scale_c(p, di, wk, coef + 4 * k);
+    }
+    /* (z^n - g^n) / (n g^(n-1)) */
+    uint32_t zn[4], s[4];
+    ext_pow_c(F, z, n, zn);
+    zn[0] = fsub(p, zn[0], fpow(p, F->generator, n));
+    uint32_t den = fmul(p, (uint32_t)(n % p), fpow(p, F->generator, n - 1));
+    ext_scale_c(p, zn, finv(p, den), s);
+#pragma omp parallel for schedule(static)
+    for (long long j = 0; j < (long long)w; j++) {
+        uint32_t acc[4] = {0, 0, 0, 0}, t[4];
+        for (uint64_t k = 0; k < n; k++) {
+            /* natural index k sits at bit-reversed position rev(k) of the prefix */
+            uint32_t y = c_from(c, lde[bitrev(k, log_n) * w + (uint64_t)j]);
+            ext_scale_c(p, coef + 4 * k, y, t);
+            ext_add_c(p, acc, t, acc);
+        }
+        ext_mul_c(p, F->w_ext, acc, s, out + 4 * j);
+    }
+    free(coef);
+    return ORC_OK;
+}
+
+static uint64_t batch_value_words(const orc_open_batch *b) {
+    uint64_t v = 0;
+    for (uint32_t m = 0; m < b->n_mats; m++) v += 4ull * b->n_points[m] * b->widths[m];
+    return v;
+}
+
+int orc_open_values(int field, const orc_open_batch *b, uint32_t log_blowup, uint32_t *values) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    const uint32_t *pt = b->points;
+    uint32_t *out = values;
+    for (uint32_t m = 0; m < b->n_mats; m++) {
+        if (b->log_heights[m] < log_blowup) return ORC_EINVAL;
+        for (uint32_t k = 0; k < b->n_points[m]; k++, pt += 4) {
+            uint32_t z[4];
+            for (int i = 0; i < 4; i++) z[i] = c_from(c, pt[i]);
+            uint32_t *o = malloc((uint64_t)b->widths[m] * 16 + 16);
+            if (!o) return ORC_ENOMEM;
+            int rc = open_one(F, c, field, b->ldes[m], b->log_heights[m], b->widths[m], log_blowup, z, o);
+            if (rc) { free(o); return rc; }
+            for (uint64_t i = 0; i < 4ull * b->widths[m]; i++) out[i] = c_to(c, o[i]);
+            out += 4ull * b->widths[m];
+            free(o);
+        }
+    }
+    return ORC_OK;
+}
+
+/* Reduced openings: ro[h] (2^h x 4, canonical) for every LDE height h of a
+ * matrix, zero where no point is opened; alpha canonical, values Monty. */
+static int reduce_openings(const field_t *F, conv_t c, int field, const orc_open_batch *batches,
+                           uint32_t n_batches, const uint32_t *values, const uint32_t *alpha, uint32_t **ro) {
+    uint32_t p = F->p;
+    uint64_t num_reduced[32] = {0};
+    /* distinct points and the tallest height each is opened at */
+    uint32_t n_pts = 0, cap = 16;
+    uint32_t (*pts)[4] = malloc(cap * 16);
+    uint32_t *pt_log = malloc(cap * 4);
+    uint32_t **dinv = NULL;
+    int rc = ORC_OK;
+    if (!pts || !pt_log) { rc = ORC_ENOMEM; goto out; }
+    for (uint32_t b = 0; b < n_batches; b++) {
+        const uint32_t *pt = batches[b].points;
+        for (uint32_t m = 0; m < batches[b].n_mats; m++)
+            for (uint32_t k = 0; k < batches[b].n_points[m]; k++, pt += 4) {
+                uint32_t z[4];
+                for (int i = 0; i < 4; i++) z[i] = c_from(c, pt[i]);
+                uint32_t q = 0;
+                while (q < n_pts && memcmp(pts[q], z, 16) != 0) q++;
+                if (q == n_pts) {
+                    if (n_pts == cap) {
+                        cap *= 2;
+                        void *a = realloc(pts, cap * 16), *l = realloc(pt_log, cap * 4);
+                        if (a) pts = a;
+                        if (l) pt_log = l;
+                        if (!a || !l) { rc = ORC_ENOMEM; goto out; }
+                    }
+                    memcpy(pts[q], z, 16);
+                    pt_log[q] = 0;
+                    n_pts++;
+                }
+                if (batches[b].log_heights[m] > pt_log[q]) pt_log[q] = batches[b].log_heights[m];
+            }
+    }
+    /* 1 / (z - x_i) over the tallest height of each point; shorter heights use
+     * a prefix (bit-reversed order nests the subgroups). */
+    dinv = calloc(n_pts ? n_pts : 1, sizeof(uint32_t *));
+    if (!dinv) { rc = ORC_ENOMEM; goto out; }
+    for (uint32_t q = 0; q < n_pts; q++) {
+        uint64_t N = 1ull << pt_log[q];
+        dinv[q] = malloc(N * 16);
+        if (!dinv[q]) { rc = ORC_ENOMEM; goto out; }
+        uint32_t wh = orc_two_adic_generator(field, pt_log[q]);
+        const uint32_t *z = pts[q];
+        uint32_t *dq = dinv[q];
+        uint32_t lq = pt_log[q];
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)N; i++) {
+            uint32_t d[4];
+            memcpy(d, z, 16);
+            d[0] = fsub(p, d[0], lde_point(F, wh, lq, (uint64_t)i));
+            ext_inv_c(F, d, dq + 4 * i);
+        }
+    }
+    const uint32_t *val = values;
+    for (uint32_t b = 0; b < n_batches; b++) {
+        const orc_open_batch *B = &batches[b];
+        const uint32_t *pt = B->points;
+        for (uint32_t m = 0; m < B->n_mats; m++) {
+            uint32_t h = B->log_heights[m], w = B->widths[m];
+            uint64_t N = 1ull << h;
+            if (!ro[h]) {
+                ro[h] = calloc(N * 4, sizeof(uint32_t));
+                if (!ro[h]) { rc = ORC_ENOMEM; goto out; }
+            }
+            if (B->n_points[m] == 0) continue;
+            /* alpha^j for the row reduction */
+            uint32_t *apow = malloc(((uint64_t)w + 1) * 16);
+            uint32_t *rr = malloc(N * 16);
+            if (!apow || !rr) { free(apow); free(rr); rc = ORC_ENOMEM; goto out; }
+            apow[0] = 1; apow[1] = apow[2] = apow[3] = 0;
+            for (uint32_t j = 1; j <= w; j++) ext_mul_c(p, F->w_ext, apow + 4 * (j - 1), alpha, apow + 4 * j);
+            const uint32_t *M = B->ldes[m];
+#pragma omp parallel for schedule(static)
+            for (long long i = 0; i < (long long)N; i++) {
+                uint32_t acc[4] = {0, 0, 0, 0}, t[4];
+                for (uint32_t j = 0; j < w; j++) {
+                    ext_scale_c(p, apow + 4 * j, c_from(c, M[(uint64_t)i * w + j]), t);
+                    ext_add_c(p, acc, t, acc);
+                }
+                memcpy(rr + 4 * i, acc, 16);
+            }
+            for (uint32_t k = 0; k < B->n_points[m]; k++, pt += 4) {
+                uint32_t z[4], rys[4] = {0, 0, 0, 0}, aoff[4], t[4];
+                for (int i = 0; i < 4; i++) z[i] = c_from(c, pt[i]);
+                uint32_t q = 0;
+                while (memcmp(pts[q], z, 16) != 0) q++;
+                for (uint32_t j = 0; j < w; j++) {
+                    uint32_t y[4];
+                    for (int i = 0; i < 4; i++) y[i] = c_from(c, val[4 * j + i]);
+                    ext_mul_c(p, F->w_ext, apow + 4 * j, y, t);
+                    ext_add_c(p, rys, t, rys);
+                }
+                ext_pow_c(F, alpha, num_reduced[h], aoff);
+                const uint32_t *dq = dinv[q];
+                uint32_t *roh = ro[h];
+#pragma omp parallel for schedule(static)
+                for (long long i = 0; i < (long long)N; i++) {
+                    uint32_t u[4];
+                    ext_sub_c(p, rys, rr + 4 * i, u);
+                    ext_mul_c(p, F->w_ext, u, aoff, u);
+                    ext_mul_c(p, F->w_ext, u, dq + 4 * i, u);
+                    ext_add_c(p, roh + 4 * i, u, roh + 4 * i);
+                }
+                num_reduced[h] += w;
+                val += 4ull * w;
+            }
+            free(apow);
+            free(rr);
+        }
+    }
+out:
+    if (dinv)
+        for (uint32_t q = 0; q < n_pts; q++) free(dinv[q]);
+    free(dinv);
+    free(pts);
+    free(pt_log);
+    return rc;
+}
+
+int orc_reduce_openings(int field, const orc_open_batch *batches, uint32_t n_batches, const uint32_t *values,
+                        const uint32_t alpha[4], uint32_t log_height, uint32_t *ro_out) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    uint32_t *ro[32] = {0}, a[4];
+    for (int i = 0; i < 4; i++) a[i] = c_from(c, alpha[i]);
+    int rc = reduce_openings(F, c, field, batches, n_batches, values, a, ro);
+    if (rc == ORC_OK) {
+        if (log_height >= 32 || !ro[log_height]) rc = ORC_EINVAL;
+        else
+            for (uint64_t i = 0; i < (4ull << log_height); i++) ro_out[i] = c_to(c, ro[log_height][i]);
+    }
+    for (int h = 0; h < 32; h++) free(ro[h]);
+    return rc;
+}
+
+static uint32_t batch_log_max(const orc_open_batch *b) {
+    uint32_t l = 0;
+    for (uint32_t m = 0; m < b->n_mats; m++) if (b->log_heights[m] > l) l = b->log_heights[m];
+    return l;
+}
+
+uint64_t orc_open_query_words(const orc_open_batch *batches, uint32_t n_batches, uint32_t log_blowup) {
+    uint32_t log_max = 0;
+    uint64_t q = 0;
+    for (uint32_t b = 0; b < n_batches; b++) {
+        uint32_t lb = batch_log_max(&batches[b]);
+        if (lb > log_max) log_max = lb;
+        for (uint32_t m = 0; m < batches[b].n_mats; m++) q += batches[b].widths[m];
+        q += 8ull * lb;
+    }
+    for (uint32_t L = log_max; L > log_blowup; L--) q += 4 + 8ull * (L - 1);
+    return q;
+}
+
+/* First witness w (ascending) with sample_bits(bits) == 0 after observing it. */
+static uint32_t grind(int field, const orc_challenger *ch, uint32_t bits) {
+    const field_t *F = fld(field);
+    const uint32_t mask = (bits >= 32) ? 0xffffffffu : ((1u << bits) - 1u);
+    const uint32_t chunk = 1u << 14;
+    uint8_t *ok = malloc(chunk);
+    if (!ok) return 0xffffffffu;
+    for (uint64_t base = 0; base < F->p; base += chunk) {
+#pragma omp parallel for schedule(static)
+        for (long long k = 0; k < (long long)chunk; k++) {
+            uint64_t w = base + (uint64_t)k;
+            ok[k] = 0;
+            if (w >= F->p) continue;
+            orc_challenger t = *ch;
+            orc_challenger_observe(field, &t, orc_to_monty(field, (uint32_t)w));
+            uint32_t v = orc_from_monty(field, orc_challenger_sample(field, &t));
+            ok[k] = (v & mask) == 0;
+        }
+        for (uint32_t k = 0; k < chunk; k++)
+            if (ok[k]) { free(ok); return (uint32_t)(base + k); }
+    }
+    free(ok);
+    return 0xffffffffu;
+}
+
+static void observe_ext_monty(int field, orc_challenger *ch, const uint32_t *v) {
+    for (int i = 0; i < 4; i++) orc_challenger_observe(field, ch, v[i]);
+}
+static void sample_ext_monty(int field, orc_challenger *ch, uint32_t *v) {
+    for (int i = 0; i < 4; i++) v[i] = orc_challenger_sample(field, ch);
+}
+
+int orc_pcs_open(int field, const orc_open_batch *batches, uint32_t n_batches, uint32_t log_blowup,
+                 uint32_t num_queries, uint32_t pow_bits, orc_challenger *ch, uint32_t *values,
+                 uint32_t *roots, uint32_t *betas, uint32_t final_poly[4], uint32_t *pow_witness,
+                 uint32_t *indices, uint32_t *queries, uint32_t *rounds_out) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    uint32_t p = F->p;
+    if (n_batches == 0) return ORC_EINVAL;
+    uint32_t log_max = 0;
+    for (uint32_t b = 0; b < n_batches; b++) {
+        if (batches[b].n_mats == 0) return ORC_EINVAL;
+        uint32_t lb = batch_log_max(&batches[b]);
+        if (lb > log_max) log_max = lb;
+    }
+    if (log_max <= log_blowup || log_max > F->two_adicity) return ORC_EINVAL;
+    /* 1. opened values, observed in order; alpha */
+    uint64_t voff = 0;
+    for (uint32_t b = 0; b < n_batches; b++) {
+        int rc = orc_open_values(field, &batches[b], log_blowup, values + voff);
+        if (rc) return rc;
+        voff += batch_value_words(&batches[b]);
+    }
+    for (uint64_t i = 0; i < voff; i++) orc_challenger_observe(field, ch, values[i]);
+    uint32_t alpha[4], ac[4];
+    sample_ext_monty(field, ch, alpha);
+    for (int i = 0; i < 4; i++) ac[i] = c_from(c, alpha[i]);
+    /* 2. reduced openings */
+    uint32_t *ro[32] = {0};
+    int rc = reduce_openings(F, c, field, batches, n_batches, values, ac, ro);
+    uint32_t R = log_max - log_blowup;
+    uint32_t **cws = calloc(R + 1, sizeof(uint32_t *)), **lay = calloc(R + 1, sizeof(uint32_t *));
+    if (!rc && (!cws || !lay)) rc = ORC_ENOMEM;
+    /* 3. commit phase */
+    uint32_t *cur = NULL;
+    if (!rc) {
+        uint64_t len = 1ull << log_max;
+        cur = malloc(len * 16);
+        if (!cur) rc = ORC_ENOMEM;
+        else memcpy(cur, ro[log_max], len * 16);
+        for (uint32_t r = 0; !rc && r < R; r++) {
+            uint64_t h = len / 2;
+            cws[r] = malloc(len * 16);
+            lay[r] = malloc((2 * h - 1) * 32);
+            uint32_t *nxt = malloc(h * 16);
+            if (!cws[r] || !lay[r] || !nxt) { free(nxt); rc = ORC_ENOMEM; break; }
+            for (uint64_t i = 0; i < len * 4; i++) cws[r][i] = c_to(c, cur[i]);
+            const uint32_t *mats[1] = {cws[r]};
+            uint64_t hh[1] = {h};
+            uint32_t ww[1] = {8};
+            uint32_t root[8], beta[4], bc[4];
+            rc = orc_mmcs_commit(field, 1, mats, hh, ww, root, lay[r]);
+            if (rc) { free(nxt); break; }
+            if (roots) memcpy(roots + 8 * r, root, 32);
+            for (int i = 0; i < 8; i++) orc_challenger_observe(field, ch, root[i]);
+            sample_ext_monty(field, ch, beta);
+            if (betas) memcpy(betas + 4 * r, beta, 16);
+            for (int i = 0; i < 4; i++) bc[i] = c_from(c, beta[i]);
+            fri_fold(F, cur, len, bc, nxt);
+            free(cur);
+            cur = nxt;
+            len = h;
+            uint32_t lh = log_max - r - 1;
+            if (ro[lh])
+                for (uint64_t i = 0; i < len * 4; i++) cur[i] = fadd(p, cur[i], ro[lh][i]);
+        }
+        if (!rc) {
+            for (uint64_t i = 1; i < len && !rc; i++)
+                if (memcmp(cur + 4 * i, cur, 16) != 0) rc = ORC_EINVAL; /* not of low degree */
+        }
+        if (!rc) {
+            uint32_t fm[4];
+            for (int i = 0; i < 4; i++) fm[i] = c_to(c, cur[i]);
+            if (final_poly) memcpy(final_poly, fm, 16);
+            observe_ext_monty(field, ch, fm);
+        }
+    }
+    /* 4. proof of work, query indices */
+    if (!rc) {
+        uint32_t w = grind(field, ch, pow_bits);
+        if (w == 0xffffffffu) rc = ORC_EINVAL;
+        else {
+            if (pow_witness) *pow_witness = orc_to_monty(field, w);
+            orc_challenger_observe(field, ch, orc_to_monty(field, w));
+            (void)orc_challenger_sample(field, ch);
+        }
+    }
+    uint64_t qw = orc_open_query_words(batches, n_batches, log_blowup);
+    for (uint32_t q = 0; !rc && q < num_queries; q++) {
+        uint32_t v = orc_from_monty(field, orc_challenger_sample(field, ch));
+        uint64_t idx = v & (uint32_t)((1ull << log_max) - 1);
+        if (indices) indices[q] = (uint32_t)idx;
+        if (!queries) continue;
+        uint32_t *rec = queries + q * qw;
+        for (uint32_t b = 0; b < n_batches; b++) {
+            const orc_open_batch *B = &batches[b];
+            uint32_t lb = batch_log_max(B);
+            uint64_t ib = idx >> (log_max - lb);
+            for (uint32_t m = 0; m < B->n_mats; m++) {
+                uint64_t row = ib >> (lb - B->log_heights[m]);
+                memcpy(rec, B->ldes[m] + row * B->widths[m], 4ull * B->widths[m]);
+                rec += B->widths[m];
+            }
+            uint64_t loff = 0;
+            for (uint32_t l = 0; l < lb; l++) {
+                uint64_t sib = (ib >> l) ^ 1;
+                memcpy(rec, B->layers + (loff + sib) * 8, 32);
+                rec += 8;
+                loff += 1ull << (lb - l);
+            }
+        }
+        for (uint32_t r = 0; r < R; r++) {
+            uint32_t L = log_max - r;
+            uint64_t ir = idx >> r;
+            memcpy(rec, cws[r] + (ir ^ 1) * 4, 16);
+            rec += 4;
+            uint64_t pair = ir >> 1, loff = 0;
+            for (uint32_t l = 0; l + 1 < L; l++) {
+                uint64_t sib = (pair >> l) ^ 1;
+                memcpy(rec, lay[r] + (loff + sib) * 8, 32);
+                rec += 8;
+                loff += 1ull << (L - 1 - l);
+            }
+        }
+    }
+    if (rounds_out) *rounds_out = R;
+    free(cur);
+    if (cws) for (uint32_t r = 0; r <= R; r++) free(cws[r]);
+    if (lay) for (uint32_t r = 0; r <= R; r++) free(lay[r]);
+    free(cws);
+    free(lay);
+    for (int h = 0; h < 32; h++) free(ro[h]);
+    return rc;
+}
+
+/* ---------------- verifier (fri.rs:77-436), for tests ---------------- */
+/* verify_batch (fri.rs:389-436): rows in input order, canonical digests. */
+static int verify_batch_c(const field_t *F, conv_t c, const uint32_t *root_monty, uint32_t n,
+                          const uint32_t *log_heights, const uint32_t *widths, const uint32_t *const *rows,
+                          uint64_t index, const uint32_t *path, uint32_t path_len) {
+    uint32_t order[64];
+    if (n == 0 || n > 64) return 0;
+    for (uint32_t i = 0; i < n; i++) order[i] = i;
+    for (uint32_t i = 1; i < n; i++) {
+        uint32_t v = order[i];
+        int j = (int)i - 1;
+        while (j >= 0 && log_heights[order[j]] < log_heights[v]) { order[j + 1] = order[j]; j--; }
+        order[j + 1] = v;
+    }
+    uint32_t pos = 0, cur_h = log_heights[order[0]];
+    sponge_t sp;
+    sponge_init(&sp);
+    while (pos < n && log_heights[order[pos]] == cur_h) {
+        for (uint32_t j = 0; j < widths[order[pos]]; j++) sponge_absorb(F, &sp, c_from(c, rows[order[pos]][j]));
+        pos++;
+    }
+    uint32_t d[8];
+    sponge_finish(F, &sp, d);
+    for (uint32_t l = 0; l < path_len; l++) {
+        uint32_t sib[8];
+        for (int i = 0; i < 8; i++) sib[i] = c_from(c, path[8 * l + i]);
+        if ((index >> l) & 1) compress_canon(F, sib, d, d);
+        else compress_canon(F, d, sib, d);
+        cur_h--;
+        if (pos < n && log_heights[order[pos]] == cur_h) {
+            sponge_init(&sp);
+            while (pos < n && log_heights[order[pos]] == cur_h) {
+                for (uint32_t j = 0; j < widths[order[pos]]; j++)
+                    sponge_absorb(F, &sp, c_from(c, rows[order[pos]][j]));
+                pos++;
+            }
+            uint32_t rd[8];
+            sponge_finish(F, &sp, rd);
+            compress_canon(F, d, rd, d);
+        }
+    }
+    for (int i = 0; i < 8; i++)
+        if (c_to(c, d[i]) != root_monty[i]) return 0;
+    return 1;
+}
+
+int orc_verify_open(int field, const orc_open_batch *batches, uint32_t n_batches, uint32_t log_blowup,
+                    uint32_t num_queries, uint32_t pow_bits, orc_challenger *ch, const uint32_t *values,
+                    const uint32_t *roots, uint32_t n_rounds, const uint32_t final_poly[4], uint32_t pow_witness,
+                    const uint32_t *queries, uint32_t *indices_out) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    uint32_t p = F->p;
+    uint64_t nv = 0;
+    for (uint32_t b = 0; b < n_batches; b++) nv += batch_value_words(&batches[b]);
+    for (uint64_t i = 0; i < nv; i++) orc_challenger_observe(field, ch, values[i]);
+    uint32_t alpha[4], beta[64][4];
+    sample_ext_monty(field, ch, alpha);
+    if (n_rounds > 64) return ORC_EINVAL;
+    for (uint32_t r = 0; r < n_rounds; r++) {
+        for (int i = 0; i < 8; i++) orc_challenger_observe(field, ch, roots[8 * r + i]);
+        sample_ext_monty(field, ch, beta[r]);
+    }
+    observe_ext_monty(field, ch, final_poly);
+    orc_challenger_observe(field, ch, pow_witness);
+    uint32_t pw = orc_from_monty(field, orc_challenger_sample(field, ch));
+    if (pow_bits && (pw & ((1u << pow_bits) - 1u))) return 10; /* proof of work */
+    uint32_t log_max = n_rounds + log_blowup;
+    uint32_t ac[4], fc[4];
+    for (int i = 0; i < 4; i++) { ac[i] = c_from(c, alpha[i]); fc[i] = c_from(c, final_poly[i]); }
+    uint64_t qw = orc_open_query_words(batches, n_batches, log_blowup);
+    for (uint32_t q = 0; q < num_queries; q++) {
+        uint64_t idx = orc_from_monty(field, orc_challenger_sample(field, ch)) & (uint32_t)((1ull << log_max) - 1);
+        if (indices_out) indices_out[q] = (uint32_t)idx;
+        const uint32_t *rec = queries + q * qw;
+        uint32_t ro[32][4];
+        memset(ro, 0, sizeof ro);
+        uint32_t pow_h[32] = {0};
+        const uint32_t *val = values;
+        for (uint32_t b = 0; b < n_batches; b++) {
+            const orc_open_batch *B = &batches[b];
+            uint32_t lb = batch_log_max(B);
+            if (B->n_mats > 64) return ORC_EINVAL;
+            const uint32_t *rows[64];
+            for (uint32_t m = 0; m < B->n_mats; m++) { rows[m] = rec; rec += B->widths[m]; }
+            uint64_t ib = idx >> (log_max - lb);
+            if (!verify_batch_c(F, c, B->root, B->n_mats, B->log_heights, B->widths, rows, ib, rec, lb))
+                return 11; /* input batch opening */
+            rec += 8ull * lb;
+            const uint32_t *pt = B->points;
+            for (uint32_t m = 0; m < B->n_mats; m++) {
+                uint32_t h = B->log_heights[m];
+                uint64_t ih = idx >> (log_max - h);
+                uint32_t x = lde_point(F, orc_two_adic_generator(field, h), h, ih);
+                for (uint32_t k = 0; k < B->n_points[m]; k++, pt += 4) {
+                    uint32_t acc[4] = {0, 0, 0, 0}, z[4], t[4], ap[4];
+                    for (uint32_t j = 0; j < B->widths[m]; j++) {
+                        for (int i = 0; i < 4; i++) t[i] = c_from(c, val[4 * j + i]);
+                        t[0] = fsub(p, t[0], c_from(c, rows[m][j]));
+                        ext_pow_c(F, ac, pow_h[h]++, ap);
+                        ext_mul_c(p, F->w_ext, t, ap, t);
+                        ext_add_c(p, acc, t, acc);
+                    }
+                    val += 4ull * B->widths[m];
+                    for (int i = 0; i < 4; i++) z[i] = c_from(c, pt[i]);
+                    z[0] = fsub(p, z[0], x);
+                    ext_inv_c(F, z, z);
+                    ext_mul_c(p, F->w_ext, acc, z, t);
+                    ext_add_c(p, ro[h], t, ro[h]);
+                }
+            }
+        }
+        if (ro[log_blowup][0] | ro[log_blowup][1] | ro[log_blowup][2] | ro[log_blowup][3]) return 12;
+        /* verify_query (fri.rs:288-387) */
+        uint32_t folded[4] = {0, 0, 0, 0};
+        uint32_t x = fpow(p, orc_two_adic_generator(field, log_max), bitrev(idx, log_max));
+        for (uint32_t r = 0; r < n_rounds; r++) {
+            uint32_t lf = log_max - 1 - r;
+            ext_add_c(p, folded, ro[lf + 1], folded);
+            uint32_t bit = (uint32_t)((idx >> r) & 1);
+            uint32_t sib[4], e0[4], e1[4];
+            for (int i = 0; i < 4; i++) sib[i] = c_from(c, rec[i]);
+            rec += 4;
+            if (bit) { memcpy(e0, sib, 16); memcpy(e1, folded, 16); }
+            else { memcpy(e0, folded, 16); memcpy(e1, sib, 16); }
+            uint32_t row[8], lh[1] = {lf}, wd[1] = {8};
+            for (int i = 0; i < 4; i++) { row[i] = c_to(c, e0[i]); row[4 + i] = c_to(c, e1[i]); }
+            const uint32_t *rp[1] = {row};
+            if (!verify_batch_c(F, c, roots + 8 * r, 1, lh, wd, rp, idx >> (r + 1), rec, lf)) return 13;
+            rec += 8ull * lf;
+            uint32_t x0 = bit ? fsub(p, 0, x) : x, x1 = bit ? x : fsub(p, 0, x);
+            uint32_t d[4], bm[4];
+            ext_sub_c(p, e1, e0, d);
+            ext_scale_c(p, d, finv(p, fsub(p, x1, x0)), d);
+            for (int i = 0; i < 4; i++) bm[i] = c_from(c, beta[r][i]);
+            bm[0] = fsub(p, bm[0], x0);
+            ext_mul_c(p, F->w_ext, bm, d, d);
+            ext_add_c(p, e0, d, folded);
+            x = fmul(p, x, x);
+        }
+        if (memcmp(folded, fc, 16) != 0) return 14;
+    }
+    return ORC_OK;
+}

@@ -114,6 +114,52 @@ int orc_fri_commit_phase(int field, const uint32_t *codeword, uint32_t log_n,
 
 /* Extension-field helpers (Monty in/out), for tests. */
 void orc_ext_mul(int field, const uint32_t a[4], const uint32_t b[4], uint32_t out[4]);
+void orc_ext_inv(int field, const uint32_t a[4], uint32_t out[4]);
+
+/*
+ * One batch of TwoAdicFriPcs::open: a committed batch and, per matrix, the
+ * points it is opened at.  Prover fields: ldes (bit-reversed LDE rows, Monty)
+ * and layers (the batch's digest layers as orc_mmcs_commit writes them).
+ * Verifier field: root.  Points are degree-4 extension elements (4 Monty
+ * words each), concatenated in matrix order.
+ */
+typedef struct {
+    uint32_t n_mats;
+    const uint32_t *const *ldes;
+    const uint32_t *log_heights; /* log2 of the LDE heights */
+    const uint32_t *widths;
+    const uint32_t *n_points;
+    const uint32_t *points;
+    const uint32_t *layers;
+    const uint32_t *root;
+} orc_open_batch;
+
+/* Opened values p_m(z) of one batch, ordered matrix, point, column (4 words each). */
+int orc_open_values(int field, const orc_open_batch *b, uint32_t log_blowup, uint32_t *values);
+/* The reduced opening of LDE height 2^log_height (2^log_height x 4 words). */
+int orc_reduce_openings(int field, const orc_open_batch *batches, uint32_t n_batches, const uint32_t *values,
+                        const uint32_t alpha[4], uint32_t log_height, uint32_t *ro_out);
+/* Words of one query record (see orc_pcs_open). */
+uint64_t orc_open_query_words(const orc_open_batch *batches, uint32_t n_batches, uint32_t log_blowup);
+/*
+ * TwoAdicFriPcs::open: opened values, alpha, reduced openings, FRI commit phase
+ * with the shorter reduced openings added at their heights, proof-of-work
+ * witness (the smallest that passes), query indices and query records.
+ * A query record holds, for each batch, the opened row of every matrix (input
+ * order) and the batch's Merkle path (leaf level first); then, for each FRI
+ * round, the sibling value (4 words) and the path in that round's tree.
+ */
+int orc_pcs_open(int field, const orc_open_batch *batches, uint32_t n_batches, uint32_t log_blowup,
+                 uint32_t num_queries, uint32_t pow_bits, orc_challenger *ch, uint32_t *values,
+                 uint32_t *roots, uint32_t *betas, uint32_t final_poly[4], uint32_t *pow_witness,
+                 uint32_t *indices, uint32_t *queries, uint32_t *rounds_out);
+/* The Pico verifier's checks on an opening proof; 0 when it verifies, else
+ * the failing check (10 proof of work, 11 input batch path, 12 reduced
+ * opening at the blowup height, 13 commit-phase path, 14 final polynomial). */
+int orc_verify_open(int field, const orc_open_batch *batches, uint32_t n_batches, uint32_t log_blowup,
+                    uint32_t num_queries, uint32_t pow_bits, orc_challenger *ch, const uint32_t *values,
+                    const uint32_t *roots, uint32_t n_rounds, const uint32_t final_poly[4], uint32_t pow_witness,
+                    const uint32_t *queries, uint32_t *indices_out);
 
 #ifdef __cplusplus
 }
