@@ -201,6 +201,72 @@ pico_status pico_gpu_fri_release(pico_ctx *ctx, pico_fri *f);
 /* Codeword of round r (r = 0 is the input) as 2^(log_n - r) x 4 words. */
 pico_status pico_gpu_fri_layer(pico_ctx *ctx, const pico_fri *f, uint32_t round, uint32_t *out, uint32_t flags);
 
+/* ---- PCS opening (TwoAdicFriPcs::open, vm/src/machine/prover.rs:589) -------
+ * Every step follows the Pico verifier (vm/src/compiler/recursion/circuit/
+ * fri.rs:77-436): opened values p(z) by barycentric evaluation over each
+ * matrix's low coset; all of them observed (4 coefficients each, batch /
+ * matrix / point / column order), then alpha sampled; one reduced opening
+ * per LDE height; the FRI commit phase folds the tallest one and adds each
+ * shorter one at its height; the final element is observed, a proof-of-work
+ * witness found (the smallest that passes), and the query indices sampled.
+ *
+ * One batch: a resident commitment (committed with the same log_blowup) and,
+ * for each of its matrices in commit input order, the points it is opened at
+ * (degree-4 extension elements, 4 Monty words each, concatenated in matrix
+ * order; n_points[m] may be 0). */
+typedef struct {
+  const pico_commit *commit;
+  const uint32_t *n_points;
+  const uint32_t *points;
+} pico_open_batch;
+
+typedef struct {
+  uint32_t log_blowup;
+  uint32_t num_queries;
+  uint32_t proof_of_work_bits; /* at most 24 */
+  uint32_t reserved;
+} pico_fri_params;
+
+typedef struct {
+  float ms_values;  /* device: inverse denominators and opened values */
+  float ms_reduce;  /* device: reduced openings */
+  float ms_fri;     /* device: commit phase */
+  float ms_grind;   /* device: proof of work */
+  float ms_queries; /* device: query records */
+  float ms_total;   /* wall clock of the call */
+  uint64_t value_cells;  /* low-coset cells read per opened point */
+  uint64_t reduce_cells; /* committed cells read by the reduction */
+  uint32_t launches;
+  uint32_t rounds;
+} pico_open_stats;
+
+/* Output sizes: opened-value words (sum of n_points x width x 4), FRI rounds
+ * (log of the tallest LDE height - log_blowup) and words per query record. */
+pico_status pico_gpu_open_sizes(const pico_open_batch *batches, uint32_t n_batches, uint32_t log_blowup,
+                                uint64_t *value_words, uint32_t *rounds, uint64_t *query_words);
+
+/* The whole opening.  ch: the prover's challenger (in/out).  Outputs (host):
+ * values (value_words), commit_roots (rounds x 8), betas (rounds x 4,
+ * nullable), final_poly (4), pow_witness (1, Monty), query_indices
+ * (num_queries), queries (num_queries x query_words): per query, for each
+ * batch the opened row of every matrix (input order) then the batch's Merkle
+ * path (leaf level first); then for each FRI round the sibling value (4
+ * words) and the path in that round's tree.  stats nullable. */
+pico_status pico_gpu_pcs_open(pico_ctx *ctx, const pico_open_batch *batches, uint32_t n_batches,
+                              const pico_fri_params *params, pico_challenger *ch, uint32_t *values,
+                              uint32_t *commit_roots, uint32_t *betas, uint32_t final_poly[4], uint32_t *pow_witness,
+                              uint32_t *query_indices, uint32_t *queries, pico_open_stats *stats);
+
+/* The first step alone: opened values (value_words), no transcript. */
+pico_status pico_gpu_open_values(pico_ctx *ctx, const pico_open_batch *batches, uint32_t n_batches,
+                                 uint32_t log_blowup, uint32_t *values);
+
+/* The reduced opening of LDE height 2^log_height (2^log_height x 4 words) for
+ * the given opened values and alpha, as fed to the commit phase. */
+pico_status pico_gpu_reduced_opening(pico_ctx *ctx, const pico_open_batch *batches, uint32_t n_batches,
+                                     uint32_t log_blowup, const uint32_t *values, const uint32_t alpha[4],
+                                     uint32_t log_height, uint32_t *out);
+
 /* ---- serving: asynchronous commits ----------------------------------------
  * pico_gpu_submit_commit copies the host matrices it is given before it
  * returns (the caller may reuse them) and queues the commit.  A request is

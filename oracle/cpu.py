@@ -233,18 +233,25 @@ def ext_inv(field: int, a) -> np.ndarray:
 
 class _Batches:
     """ctypes view of opening batches.  Each batch is a dict with `ldes`
-    (committed LDEs, bit-reversed rows, Monty), `points` (per matrix an array
-    of shape (k, 4)), and optionally `layers` and `root`."""
+    (committed LDEs, bit-reversed rows, Monty) -- or, for the verifier alone,
+    `shapes` [(LDE height, width)] --, `points` (per matrix an array of shape
+    (k, 4)), and optionally `layers` and `root`."""
 
     def __init__(self, batches):
         self.keep = []
         arr = (OpenBatch * len(batches))()
         for b, B in enumerate(batches):
-            ldes = [_u32(m) for m in B["ldes"]]
-            n = len(ldes)
-            ptrs = (C.c_void_p * n)(*[m.ctypes.data for m in ldes])
-            logh = np.array([m.shape[0].bit_length() - 1 for m in ldes], dtype=np.uint32)
-            widths = np.array([m.shape[1] for m in ldes], dtype=np.uint32)
+            if "ldes" in B:
+                ldes = [_u32(m) for m in B["ldes"]]
+                shapes = [m.shape for m in ldes]
+                ptrs = (C.c_void_p * len(ldes))(*[m.ctypes.data for m in ldes])
+            else:  # verifier only: LDE shapes without data
+                ldes = None
+                shapes = B["shapes"]
+                ptrs = (C.c_void_p * len(shapes))()
+            n = len(shapes)
+            logh = np.array([h.bit_length() - 1 for h, _ in shapes], dtype=np.uint32)
+            widths = np.array([w for _, w in shapes], dtype=np.uint32)
             pts = [np.asarray(P, dtype=np.uint32).reshape(-1, 4) for P in B["points"]]
             npts = np.array([len(P) for P in pts], dtype=np.uint32)
             flat = _u32(np.concatenate(pts) if sum(len(P) for P in pts) else np.zeros((1, 4), np.uint32))
@@ -257,8 +264,10 @@ class _Batches:
                                root.ctypes.data if root is not None else None)
         self.arr = arr
         self.n = len(batches)
-        self.value_words = sum(4 * len(P) * m.shape[1] for B in batches for m, P in zip(B["ldes"], B["points"])
-                               if len(np.asarray(P)))
+        self.value_words = sum(4 * len(np.asarray(P).reshape(-1, 4)) * w
+                               for B in batches
+                               for (_, w), P in zip(B["shapes"] if "shapes" in B else [m.shape for m in B["ldes"]],
+                                                    B["points"]))
 
 
 def open_values(field: int, batch, log_blowup: int) -> np.ndarray:

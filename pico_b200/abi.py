@@ -91,6 +91,37 @@ class CommitStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class OpenBatch(C.Structure):
+    _fields_ = [("commit", C.c_void_p), ("n_points", C.c_void_p), ("points", C.c_void_p)]
+
+
+class FriParams(C.Structure):
+    _fields_ = [
+        ("log_blowup", C.c_uint32),
+        ("num_queries", C.c_uint32),
+        ("proof_of_work_bits", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class OpenStats(C.Structure):
+    _fields_ = [
+        ("ms_values", C.c_float),
+        ("ms_reduce", C.c_float),
+        ("ms_fri", C.c_float),
+        ("ms_grind", C.c_float),
+        ("ms_queries", C.c_float),
+        ("ms_total", C.c_float),
+        ("value_cells", C.c_uint64),
+        ("reduce_cells", C.c_uint64),
+        ("launches", C.c_uint32),
+        ("rounds", C.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _u32p = C.POINTER(C.c_uint32)
 _vp = C.c_void_p
 _u32 = C.c_uint32
@@ -130,6 +161,15 @@ SIGNATURES = {
     "pico_gpu_request_free": (C.c_int, [_vp, _vp]),
     "pico_gpu_autotune": (C.c_int, [_vp, C.c_int, _u32, _u32, C.POINTER(C.c_float)]),
     "pico_gpu_lde_split": (C.c_int, [_vp, C.c_int, _u32, _u32, C.POINTER(_u32)]),
+    "pico_gpu_open_sizes": (C.c_int, [C.POINTER(OpenBatch), _u32, _u32, C.POINTER(_u64), C.POINTER(_u32),
+                                      C.POINTER(_u64)]),
+    "pico_gpu_pcs_open": (
+        C.c_int,
+        [_vp, C.POINTER(OpenBatch), _u32, C.POINTER(FriParams), C.POINTER(Challenger), _vp, _vp, _vp, _vp,
+         C.POINTER(_u32), _vp, _vp, C.POINTER(OpenStats)],
+    ),
+    "pico_gpu_open_values": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp]),
+    "pico_gpu_reduced_opening": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp, _vp, _u32, _vp]),
 }
 
 _lib = None

@@ -12,6 +12,7 @@
 
 #include "field.cuh"
 #include "internal.h"
+#include "open.h"
 #include "runtime.h"
 #include "serving.h"
 
@@ -84,6 +85,78 @@ static void host_twiddles(std::vector<uint32_t>& t) {
 }
 
 static uint32_t field_two_adicity(int field) { return field == 0 ? 24u : 27u; }
+
+// Host Poseidon2-16 (same round structure and constants as the device
+// permutation) for the transcript steps that run on the host: observing the
+// opened values and sampling the query indices of TwoAdicFriPcs::open.
+template <class F>
+struct HostP2 {
+  uint32_t ext[8][16], inte[24], diag[16];
+  HostP2() { host_p2_constants<F>(ext, inte, diag); }
+  static uint32_t sbox(uint32_t x) {
+    using B = Fp<F>;
+    const uint32_t x2 = B::mul(x, x);
+    if (F::SBOX == 3) return B::mul(x2, x);
+    return B::mul(B::mul(x2, x2), B::mul(x2, x));  // x^7
+  }
+  static void external(uint32_t* s) {
+    using B = Fp<F>;
+    for (int i = 0; i < 16; i += 4) {
+      // [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]]
+      const uint32_t a = s[i], b = s[i + 1], c = s[i + 2], d = s[i + 3];
+      const uint32_t sum = B::add(B::add(a, b), B::add(c, d));
+      s[i] = B::add(sum, B::add(a, B::dbl(b)));
+      s[i + 1] = B::add(sum, B::add(b, B::dbl(c)));
+      s[i + 2] = B::add(sum, B::add(c, B::dbl(d)));
+      s[i + 3] = B::add(sum, B::add(d, B::dbl(a)));
+    }
+    uint32_t col[4];
+    for (int k = 0; k < 4; k++) col[k] = B::add(B::add(s[k], s[4 + k]), B::add(s[8 + k], s[12 + k]));
+    for (int i = 0; i < 16; i++) s[i] = B::add(s[i], col[i & 3]);
+  }
+  void permute(uint32_t* s) const {
+    using B = Fp<F>;
+    external(s);
+    for (int r = 0; r < 8; r++) {
+      if (r == 4)
+        for (int q = 0; q < F::ROUNDS_P; q++) {
+          s[0] = sbox(B::add(s[0], inte[q]));
+          uint32_t sum = 0;
+          for (int i = 0; i < 16; i++) sum = B::add(sum, s[i]);
+          for (int i = 0; i < 16; i++) s[i] = B::add(B::mul(s[i], diag[i]), sum);
+        }
+      for (int j = 0; j < 16; j++) s[j] = sbox(B::add(s[j], ext[r][j]));
+      external(s);
+    }
+  }
+};
+
+void host_permute(int field, uint32_t s[16]) {
+  static const HostP2<KoalaBear> kb;
+  static const HostP2<BabyBear> bb;
+  if (field == 0)
+    kb.permute(s);
+  else
+    bb.permute(s);
+}
+
+// DuplexChallenger<F, Perm, 16, 8> (challenger.rs:89-115).
+static void host_duplex(int field, pico_challenger* ch) {
+  for (uint32_t i = 0; i < ch->in_len; i++) ch->sponge[i] = ch->in_buf[i];
+  ch->in_len = 0;
+  host_permute(field, ch->sponge);
+  for (int i = 0; i < 8; i++) ch->out_buf[i] = ch->sponge[i];
+  ch->out_len = 8;
+}
+void host_observe(int field, pico_challenger* ch, uint32_t v) {
+  ch->out_len = 0;
+  ch->in_buf[ch->in_len++] = v;
+  if (ch->in_len == 8) host_duplex(field, ch);
+}
+uint32_t host_sample(int field, pico_challenger* ch) {
+  if (ch->in_len != 0 || ch->out_len == 0) host_duplex(field, ch);
+  return ch->out_buf[--ch->out_len];
+}
 
 }  // namespace pico
 

@@ -16,6 +16,41 @@
 
 using namespace pico;
 
+namespace pico {
+pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& tw, uint32_t log_n, uint32_t R,
+                               const std::vector<uint32_t*>& codewords, const std::vector<uint32_t*>& trees,
+                               uint32_t* d_betas, DevChallenger* d_ch, const uint32_t* const* inject) {
+  pico_status s;
+  for (uint32_t r = 0; r < R; r++) {
+    const uint32_t L = log_n - r;            // codeword length 2^L
+    const uint64_t leaves = 1ull << (L - 1);  // rows of the (len/2) x 8 matrix
+    RowGroup g;
+    memset(&g, 0, sizeof g);
+    g.n_segs = 1;
+    g.total_width = 8;
+    g.segs[0].ptr = codewords[r];
+    g.segs[0].width = 8;
+    uint32_t* layer = trees[r];
+    if ((s = cuda_status(launch_hash_rows(field, g, leaves, layer, st), "FRI leaf hashing"))) return s;
+    for (uint32_t lvl = 1; lvl < L; lvl++) {
+      const uint64_t len = leaves >> lvl;
+      uint32_t* next = layer + 2 * len * 8;
+      if ((s = cuda_status(launch_compress(field, layer, next, len, nullptr, st), "FRI compression"))) return s;
+      layer = next;
+    }
+    // layer now points at the root
+    if (d_ch)
+      if ((s = cuda_status(launch_challenger_round(field, d_ch, layer, d_betas + 4 * r, st), "challenger")))
+        return s;
+    if ((s = cuda_status(launch_fri_fold_tw(field, codewords[r], L, d_betas + 4 * r, tw, codewords[r + 1], st,
+                                            inject ? inject[r] : nullptr),
+                         "fold")))
+      return s;
+  }
+  return PICO_OK;
+}
+}  // namespace pico
+
 static pico_status fri_alloc(void** p, size_t bytes, cudaStream_t st) {
   return cuda_status(cudaMallocAsync(p, bytes ? bytes : 16, st), "device allocation");
 }
@@ -105,31 +140,9 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
       if ((s = cuda_status(cudaMemcpyAsync(d_ch, ch, sizeof *ch, cudaMemcpyHostToDevice, st), "challenger")))
         return s;
     }
-    for (uint32_t r = 0; r < R; r++) {
-      const uint32_t L = log_n - r;            // codeword length 2^L
-      const uint64_t leaves = 1ull << (L - 1);  // rows of the (len/2) x 8 matrix
-      RowGroup g;
-      memset(&g, 0, sizeof g);
-      g.n_segs = 1;
-      g.total_width = 8;
-      g.segs[0].ptr = f->codewords[r];
-      g.segs[0].width = 8;
-      uint32_t* layer = f->trees[r];
-      if ((s = cuda_status(launch_hash_rows(field, g, leaves, layer, st), "FRI leaf hashing"))) return s;
-      for (uint32_t lvl = 1; lvl < L; lvl++) {
-        const uint64_t len = leaves >> lvl;
-        uint32_t* next = layer + 2 * len * 8;
-        if ((s = cuda_status(launch_compress(field, layer, next, len, nullptr, st), "FRI compression"))) return s;
-        layer = next;
-      }
-      // layer now points at the root
-      if (!betas_in)
-        if ((s = cuda_status(launch_challenger_round(field, d_ch, layer, d_betas + 4 * r, st), "challenger")))
-          return s;
-      if ((s = cuda_status(launch_fri_fold_tw(field, f->codewords[r], L, d_betas + 4 * r, tw, f->codewords[r + 1], st),
-                           "fold")))
-        return s;
-    }
+    if ((s = enqueue_fri_rounds(field, st, tw, log_n, R, f->codewords, f->trees, d_betas, betas_in ? nullptr : d_ch,
+                                nullptr)))
+      return s;
     // Read-backs are queued after the whole loop: a copy into pageable host
     // memory blocks the calling thread until the stream reaches it.
     uint32_t* last = f->codewords[R];

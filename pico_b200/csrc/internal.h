@@ -83,8 +83,11 @@ constexpr uint32_t kStageTableWords = 16384;  // words of stage (16380 used)
 cudaError_t launch_stage_tables(int field, TwiddleTables tw, uint32_t* stage, cudaStream_t st);
 // Fold one codeword of 2^log_len EF4 elements to half length with the EF4
 // challenge at beta (device, 4 words).
+// With `inject` (2^(log_len-1) x 4 words) the folded row adds inject[r]: the
+// reduced opening of the folded height (the commit-phase loop of
+// TwoAdicFriPcs::open, mirrored by fri.rs:300-318).
 cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
-                               TwiddleTables tw, uint32_t* out, cudaStream_t st);
+                               TwiddleTables tw, uint32_t* out, cudaStream_t st, const uint32_t* inject = nullptr);
 // Coefficients of the final polynomial (2^log_keep x 4 words) from the last
 // codeword of 2^log_len EF4 elements; *err set if higher coefficients are nonzero.
 cudaError_t launch_fri_final_poly(int field, const uint32_t* cw, uint32_t log_len, uint32_t log_keep,

@@ -1,0 +1,86 @@
+// Device-side descriptors and launchers of the PCS opening (open_kernels.cu),
+// shared with the host orchestration (open_host.cu).  Not part of the ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/pico_gpu.h"
+#include "field.cuh"
+#include "internal.h"
+
+namespace pico {
+
+constexpr uint32_t kOpenMaxRows = 1024;  // low-coset rows per block of k_open_partial (log_rows <= 10)
+
+// One matrix of the opened-values pass and up to two of its points.
+struct OpenDesc {
+  const uint32_t* lde;  // committed LDE, bit-reversed rows, row-major
+  uint32_t w;
+  uint32_t log_n;       // low coset (trace) height
+  uint32_t log_rows;    // rows per block
+  uint32_t n_pts;       // 1 or 2
+  uint32_t pt[2];       // distinct-point index of each point (its 1/(z - x) table)
+  uint32_t block0;      // first block of this descriptor
+  uint32_t pad;
+  uint64_t part_off;    // EF offset of this descriptor's partial sums
+  uint64_t out_off[2];  // EF offset of each point's values in the output
+};
+
+// Reduced opening of one height.
+struct ReduceMat {
+  const uint32_t* lde;
+  uint32_t w;
+  uint32_t multi;    // 0: one point (slot, off); 1: n_terms (slot, off) terms from term0
+  uint32_t slot, off;
+  uint32_t n_terms, term0;
+};
+struct ReduceTerm {
+  uint32_t slot, off;
+};
+struct ReduceHeight {
+  uint32_t log_h;
+  uint32_t n_mats;
+  uint32_t n_slots;      // distinct points at this height handled by this launch (1..4)
+  uint32_t accumulate;   // add to ro instead of overwriting
+  const ReduceMat* mats;
+  const ReduceTerm* terms;
+  const uint4* apow;     // alpha^k, EF4
+  const uint4* dinv[4];  // 1 / (z_slot - x_i)
+  Ext4 K[4];             // sum over (m, z_slot) of alpha^off * sum_j alpha^j p_j(z)
+  uint4* ro;
+};
+
+// Pieces of a query record.
+enum : uint32_t { kSegRow = 0, kSegDigest = 1, kSegSibling = 2 };
+struct QuerySeg {
+  const uint32_t* base;
+  uint64_t level_off;  // kSegDigest: digests before this layer
+  uint32_t kind;
+  uint32_t shift;      // the record uses (index >> shift)
+  uint32_t width;      // kSegRow: row width
+  uint32_t dst;        // word offset in the record
+};
+
+cudaError_t launch_inv_denoms(int field, const uint32_t z[4], uint32_t log_h, TwiddleTables tw, uint32_t* out,
+                              cudaStream_t st);
+cudaError_t launch_open_values(int field, const OpenDesc* descs, uint32_t n_desc, uint32_t n_blocks,
+                               const uint32_t* const* dinv_tables, TwiddleTables tw, uint32_t* partial,
+                               const uint32_t* scale, uint32_t* values, cudaStream_t st);
+cudaError_t launch_reduce(int field, const ReduceHeight& h, cudaStream_t st);
+cudaError_t launch_gather_queries(const QuerySeg* segs, uint32_t n_segs, const uint32_t* indices, uint32_t n_queries,
+                                  uint64_t query_words, uint32_t* out, cudaStream_t st);
+
+// p2_kernels.cu: smallest witness in [base, base + count) whose observation
+// makes the challenger's next sample have `bits` low zero bits; atomicMin into
+// *best (left unchanged when none; blocks exit early once *best is set).
+cudaError_t launch_grind(int field, const DevChallenger* ch, uint32_t bits, uint32_t base, uint32_t count,
+                         uint32_t* best, cudaStream_t st);
+
+// Host Poseidon2 and duplex challenger (api.cu), for transcript steps that
+// run on the host between device phases.
+void host_permute(int field, uint32_t s[16]);
+void host_observe(int field, pico_challenger* ch, uint32_t v);
+uint32_t host_sample(int field, pico_challenger* ch);
+
+}  // namespace pico

@@ -5,6 +5,7 @@
 
 #include "field.cuh"
 #include "internal.h"
+#include "open.h"
 #include "poseidon2.cuh"
 
 namespace pico {
@@ -270,7 +271,7 @@ cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uin
 // g = two_adic_generator(log len), rev over log(len/2) bits.
 template <class F>
 __global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t* beta, TwiddleTables tw,
-                           uint32_t* out) {
+                           uint32_t* out, const uint32_t* inject) {
   using B = Fp<F>;
   using E = Ef<F>;
   const uint64_t h = 1ull << (log_len - 1);
@@ -292,16 +293,20 @@ __global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t*
   Ext4 pd = E::mul(hb, E::scale(dif, t));
 #pragma unroll
   for (int i = 0; i < 4; i++) res.c[i] = B::add(B::half(sum.c[i]), pd.c[i]);
+  if (inject) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(inject) + r);
+    res = E::add(res, Ext4{{v.x, v.y, v.z, v.w}});
+  }
   reinterpret_cast<uint4*>(out)[r] = make_uint4(res.c[0], res.c[1], res.c[2], res.c[3]);
 }
 
 cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
-                               TwiddleTables tw, uint32_t* out, cudaStream_t st) {
+                               TwiddleTables tw, uint32_t* out, cudaStream_t st, const uint32_t* inject) {
   uint64_t h = 1ull << (log_len - 1);
   if (field == 0)
-    k_fri_fold<KoalaBear><<<blocks_for(h, 256), 256, 0, st>>>(cw, log_len, beta, tw, out);
+    k_fri_fold<KoalaBear><<<blocks_for(h, 256), 256, 0, st>>>(cw, log_len, beta, tw, out, inject);
   else
-    k_fri_fold<BabyBear><<<blocks_for(h, 256), 256, 0, st>>>(cw, log_len, beta, tw, out);
+    k_fri_fold<BabyBear><<<blocks_for(h, 256), 256, 0, st>>>(cw, log_len, beta, tw, out, inject);
   return cudaGetLastError();
 }
 
@@ -359,6 +364,46 @@ cudaError_t launch_challenger_observe(int field, DevChallenger* ch, const uint32
     k_challenger_observe<KoalaBear><<<1, 32, 0, st>>>(ch, vals, n);
   else
     k_challenger_observe<BabyBear><<<1, 32, 0, st>>>(ch, vals, n);
+  return cudaGetLastError();
+}
+
+// Proof-of-work search (the challenger's grind; checked by check_witness,
+// challenger.rs:210-221).  Observing candidate c and sampling always permutes
+// once: the state with its pending inputs and c written over lanes
+// 0..in_len, and the sample is lane 7 of the result (the last output popped).
+// A candidate passes when the sample's canonical value has `bits` low zero
+// bits; the smallest passing candidate of the launch wins (atomicMin).
+template <class F>
+__global__ void __launch_bounds__(256) k_grind(const DevChallenger* ch, uint32_t bits, uint32_t base,
+                                               uint32_t count, uint32_t* best) {
+  using B = Fp<F>;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (*reinterpret_cast<volatile uint32_t*>(best) != 0xffffffffu) return;  // found by an earlier launch
+  if (k >= count) return;
+  const uint64_t c = (uint64_t)base + k;
+  if (c >= F::P) return;
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = ch->sponge[i];
+  const uint32_t n_in = ch->in_len;  // below 8: a full buffer is absorbed when it fills
+  for (uint32_t i = 0; i < n_in && i < 8; i++) s[i] = ch->in_buf[i];
+  const uint32_t v = B::to_monty((uint32_t)c);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    if ((uint32_t)i == n_in) s[i] = v;
+  p2_permute<F>(s);
+  const uint32_t mask = bits >= 32 ? 0xffffffffu : ((1u << bits) - 1u);
+  if ((B::from_monty(s[7]) & mask) == 0) atomicMin(best, (uint32_t)c);
+}
+
+cudaError_t launch_grind(int field, const DevChallenger* ch, uint32_t bits, uint32_t base, uint32_t count,
+                         uint32_t* best, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  const unsigned blocks = (count + 255) / 256;
+  if (field == 0)
+    k_grind<KoalaBear><<<blocks, 256, 0, st>>>(ch, bits, base, count, best);
+  else
+    k_grind<BabyBear><<<blocks, 256, 0, st>>>(ch, bits, base, count, best);
   return cudaGetLastError();
 }
 

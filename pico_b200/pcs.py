@@ -278,6 +278,29 @@ def new_challenger() -> abi.Challenger:
     return abi.Challenger()
 
 
+class _OpenBatches:
+    """ctypes view of [(ProverData, points per matrix)] for the opening calls."""
+
+    def __init__(self, rounds):
+        self.keep = []
+        self.arr = (abi.OpenBatch * len(rounds))()
+        self.n = len(rounds)
+        for b, (pd, points) in enumerate(rounds):
+            pts = [np.asarray(P, dtype=np.uint32).reshape(-1, 4) for P in points]
+            if len(pts) != pd.n_mats:
+                raise ValueError(f"batch {b}: {len(pts)} point lists for {pd.n_mats} matrices")
+            npts = np.array([len(P) for P in pts], dtype=np.uint32)
+            flat = np.ascontiguousarray(np.concatenate(pts) if npts.sum() else np.zeros((1, 4), np.uint32))
+            self.keep += [npts, flat]
+            self.arr[b] = abi.OpenBatch(pd.handle.value, npts.ctypes.data, flat.ctypes.data)
+
+    def sizes(self, log_blowup: int):
+        vw, r, qw = C.c_uint64(), C.c_uint32(), C.c_uint64()
+        abi.check(abi.load().pico_gpu_open_sizes(self.arr, self.n, log_blowup, C.byref(vw), C.byref(r),
+                                                 C.byref(qw)))
+        return vw.value, r.value, qw.value
+
+
 class TwoAdicFriPcs:
     """SC_Pcs = TwoAdicFriPcs<Val, Dft, ValMmcs, ChallengeMmcs>."""
 
@@ -341,6 +364,56 @@ class TwoAdicFriPcs:
             final.ctypes.data, C.byref(nr), C.byref(h) if keep else None))
         data = FriData(self.ctx, h, log_n) if keep else None
         return FriCommitResult(roots[:rounds], out_betas[:rounds], final, nr.value, data)
+
+    def open(self, rounds, challenger, num_queries: int = 84, proof_of_work_bits: int = 16):
+        """TwoAdicFriPcs::open over [(ProverData, points per matrix)]: returns the
+        opened values (per batch, matrix, point: (width, 4)) and the proof pieces.
+        The challenger is advanced in place, as the prover's is."""
+        ob = _OpenBatches(rounds)
+        vw, R, qw = ob.sizes(self.log_blowup)
+        values = np.zeros(max(vw, 4), dtype=np.uint32)
+        roots = np.zeros((max(R, 1), 8), dtype=np.uint32)
+        betas = np.zeros((max(R, 1), 4), dtype=np.uint32)
+        final = np.zeros(4, dtype=np.uint32)
+        wit = C.c_uint32()
+        idx = np.zeros(max(num_queries, 1), dtype=np.uint32)
+        queries = np.zeros((max(num_queries, 1), qw), dtype=np.uint32)
+        params = abi.FriParams(self.log_blowup, num_queries, proof_of_work_bits, 0)
+        st = abi.OpenStats()
+        abi.check(self.ctx.lib.pico_gpu_pcs_open(
+            self.ctx.handle, ob.arr, ob.n, C.byref(params), C.byref(challenger), values.ctypes.data, roots.ctypes.data,
+            betas.ctypes.data, final.ctypes.data, C.byref(wit), idx.ctypes.data, queries.ctypes.data, C.byref(st)))
+        return {
+            "values": values[:vw].reshape(-1, 4),
+            "roots": roots[:R],
+            "betas": betas[:R],
+            "final": final,
+            "pow_witness": wit.value,
+            "indices": idx[:num_queries],
+            "queries": queries[:num_queries],
+            "stats": st.as_dict(),
+        }
+
+
+    def open_values(self, rounds):
+        """Opened values p(z) of every matrix at each of its points, (n, 4) Monty words."""
+        ob = _OpenBatches(rounds)
+        vw, _, _ = ob.sizes(self.log_blowup)
+        values = np.zeros(max(vw, 4), dtype=np.uint32)
+        abi.check(self.ctx.lib.pico_gpu_open_values(self.ctx.handle, ob.arr, ob.n, self.log_blowup, values.ctypes.data))
+        return values[:vw].reshape(-1, 4)
+
+
+    def reduced_opening(self, rounds, values, alpha, log_height: int):
+        """The reduced opening of LDE height 2^log_height for given values and alpha."""
+        ob = _OpenBatches(rounds)
+        v = np.ascontiguousarray(values, dtype=np.uint32)
+        a = np.ascontiguousarray(alpha, dtype=np.uint32)
+        out = np.zeros((1 << log_height, 4), dtype=np.uint32)
+        abi.check(self.ctx.lib.pico_gpu_reduced_opening(self.ctx.handle, ob.arr, ob.n, self.log_blowup,
+                                                         v.ctypes.data if v.size else None, a.ctypes.data, log_height,
+                                                         out.ctypes.data))
+        return out
 
 
 class CommitRequest:
