@@ -423,6 +423,186 @@ def run_gpu(args, rank, world, local):
     return result, shapes, field, b
 
 
+# ---------------------------------------------------------------- opening leg
+OPEN_METRIC = ("opened trace cells/sec (TwoAdicFriPcs::open: opened values, reduced openings, FRI commit "
+               "phase, proof of work, query records; bit-exact)")
+
+
+def open_points(field, shapes, seed: int = 6):
+    """Pico's main-trace opening points: zeta and zeta * w_n for each trace of height n."""
+    from pico_b200 import fields as F
+
+    p = F.P[field]
+    rng = np.random.default_rng(seed)
+    zc = [int(v) for v in rng.integers(0, p, size=4)]
+    zeta = np.array([F.monty(field, v) for v in zc], dtype=np.uint32)
+    pts = []
+    for lh, _ in shapes:
+        w = F.two_adic_generator(field, lh)
+        nxt = np.array([F.monty(field, v * w % p) for v in zc], dtype=np.uint32)
+        pts.append(np.stack([zeta, nxt]))
+    return pts
+
+
+def run_cpu_open(shapes, field, b, seed, steps, warmup, seconds, nq=84, pow_bits=16):
+    """The oracle's TwoAdicFriPcs::open on a bounded sample (smallest matrices
+    first, sized by a probe to about `seconds` per run); the commit it opens is
+    made outside the timed region."""
+    from oracle import cpu as orc
+    from pico_b200 import fields as F
+
+    probe_shape = [(12, 16)]
+    pm = [F.random_matrix(field, 12, 16, 5)]
+    root, ldes, layers = orc.pcs_commit(field, pm, [F.lde_shift(field)], b, want_ldes=True, want_layers=True)
+    pb = [{"ldes": ldes, "points": open_points(field, probe_shape), "layers": layers}]
+    t = time.perf_counter()
+    orc.pcs_open(field, pb, b, nq, pow_bits)
+    fixed = time.perf_counter() - t  # proof of work and queries dominate a tiny open
+    t = time.perf_counter()
+    orc.pcs_open(field, pb, b, nq, 0)
+    rate = (16 << 12) / max(time.perf_counter() - t, 1e-6)
+    budget = rate * max(seconds - fixed, 1.0)
+    chosen, tot = [], 0
+    for lh, w in sorted(shapes, key=lambda s: s[1] << s[0]):
+        if tot + (w << lh) > budget and chosen:
+            break
+        chosen.append((lh, w))
+        tot += w << lh
+    mats = [F.random_matrix(field, lh, w, seed * 1000 + i) for i, (lh, w) in enumerate(chosen)]
+    root, ldes, layers = orc.pcs_commit(field, mats, [F.lde_shift(field)] * len(mats), b, want_ldes=True,
+                                        want_layers=True)
+    batch = [{"ldes": ldes, "points": open_points(field, chosen), "layers": layers}]
+    for _ in range(warmup):
+        orc.pcs_open(field, batch, b, nq, pow_bits)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        orc.pcs_open(field, batch, b, nq, pow_bits)
+        times.append(time.perf_counter() - t)
+    med = float(np.median(times))
+    return {"value": tot / med, "unit": UNIT, "cores": orc.num_threads(),
+            "sample": f"open of {len(chosen)} of {len(shapes)} matrices of the workload (smallest first), "
+                      f"{tot} trace cells, 2 points each, {nq} queries, {pow_bits} proof-of-work bits; "
+                      f"median of {steps} runs",
+            "seconds_per_run": med}
+
+
+OPEN_WORKLOADS = {
+    "open-kb-2^30": lambda: uneven_kb_shapes(),
+    # the same distribution at 2^25 cells (heights 2^6..2^18): for profiler captures
+    "open-kb-2^25": lambda: uneven_kb_shapes(target_log=25, lo=6, hi=18),
+}
+
+
+def run_open(args, rank, world, local):
+    """Open the uneven KoalaBear shard's commitment (2^30 trace cells, 32
+    traces) at Pico's main-trace points: every trace at zeta and zeta * w_n;
+    84 queries, 16 proof-of-work bits, log_blowup 1 (KoalaBearPoseidon2's FRI
+    configuration, vm/src/configs/stark_config/kb_poseidon2.rs:62-72).  One
+    step = one pcs.open on the resident commitment."""
+    import torch
+
+    from pico_b200 import GpuContext, TwoAdicDomain, TwoAdicFriPcs, abi
+    from pico_b200 import fields as F
+
+    field, b, nq, pow_bits = 0, 1, 84, 16
+    shapes = OPEN_WORKLOADS[args.workload]()
+    seed = replica_seed(2, rank)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    traces = [F.random_matrix_torch(field, lh, w, seed * 1000 + i, dev) for i, (lh, w) in enumerate(shapes)]
+    torch.cuda.synchronize()
+    cells = sum(w << lh for lh, w in shapes)
+    ctx = GpuContext(local)
+    if not args.no_tune:
+        heights = [lh for lh, _ in shapes]
+        ctx.autotune(field, max(12, min(heights)), max(12, max(heights)))
+    pcs = TwoAdicFriPcs(ctx, field, b)
+    doms = [TwoAdicDomain(lh) for lh, _ in shapes]
+    root, pd = pcs.commit(list(zip(doms, traces)))
+    pts = open_points(field, shapes)
+    rounds = [(pd, pts)]
+
+    def step():
+        return pcs.open(rounds, abi.Challenger(), num_queries=nq, proof_of_work_bits=pow_bits)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    outs = [step() for _ in range(args.steps)]
+    e1.record()
+    e1.synchronize()
+    clocks = sampler.stop()
+    barrier(world)
+    ms = allmax(world, e0.elapsed_time(e1))
+    st = outs[-1]["stats"]
+    proof_bytes = 4 * (outs[-1]["values"].size + outs[-1]["roots"].size + outs[-1]["queries"].size + 4 + 1 + nq)
+
+    # roofline of the reduction: committed cells read once, per row the inverse
+    # denominators of both points read and the reduced opening written
+    heights = sorted({lh + b for lh, _ in shapes})
+    red_bytes = 4 * st["reduce_cells"] + sum((1 << h) * 16 * (2 + 1) for h in heights)
+    hbm_peak, hbm_kind = peaks()
+    red_ach = red_bytes / (st["ms_reduce"] / 1e3) / 1e9
+    val_bytes = 4 * st["value_cells"] // 2 + sum(16 * (1 << lh) * 2 for lh, _ in shapes)
+
+    # e2e: commit from pinned host traces and open, per step
+    e2e = None
+    if not args.skip_e2e:
+        host = [t.cpu().pin_memory().numpy().view(np.uint32) for t in traces]
+        pd.release()
+        del traces
+        torch.cuda.empty_cache()
+
+        def e2e_step():
+            _, pdh = pcs.commit(list(zip(doms, host)))
+            out = pcs.open([(pdh, pts)], abi.Challenger(), num_queries=nq, proof_of_work_bits=pow_bits)
+            pdh.release()
+            return out
+
+        for _ in range(max(1, args.warmup - 1)):
+            e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        ms_e2e = allmax(world, (time.perf_counter() - t0) * 1e3)
+        e2e = {"value": world * cells * args.steps / (ms_e2e / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": proof_bytes + 32,
+               "ms_per_step": ms_e2e / args.steps,
+               "what": "commit from pinned host traces + open, both through the C ABI (host wall clock)"}
+    ctx.close()
+    return {
+        "metric": OPEN_METRIC, "value": job_rate(world, cells, args.steps, ms), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (Montgomery-form KoalaBear, EF4 challenges)",
+        "data": "synthetic: seeded uniform field elements; random zeta",
+        "config": {"workload": args.workload, "matrices": len(shapes), "trace_cells": cells, "log_blowup": b,
+                   "points_per_matrix": 2, "num_queries": nq, "proof_of_work_bits": pow_bits,
+                   "l2": f"committed LDEs ({8 * cells / 2**30:.2f} GiB) larger than L2 (126 MB); no flush"},
+        "gpu_launches": int(st["launches"]) * args.steps,
+        "clocks": clocks,
+        "phases_ms": {k: st[k] for k in ("ms_values", "ms_reduce", "ms_fri", "ms_grind", "ms_queries", "ms_total")},
+        "roofline": {
+            "kernel": "k_reduce (reduced openings, one launch per height)", "bound": "hbm",
+            "achieved": red_ach, "peak": hbm_peak, "unit": "GB/s", "frac": red_ach / hbm_peak, "traffic": None,
+            "algorithmic_bytes": red_bytes, "launch_ms": st["ms_reduce"],
+            "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback"},
+        "roofline_values": {
+            "kernel": "k_inv_denoms + k_open_partial + k_open_finalize (opened values)", "bound": "hbm",
+            "achieved": val_bytes / (st["ms_values"] / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+            "frac": val_bytes / (st["ms_values"] / 1e3) / 1e9 / hbm_peak, "algorithmic_bytes": val_bytes,
+            "launch_ms": st["ms_values"]},
+        "e2e": e2e,
+    }
+
+
 # ---------------------------------------------------------------- FRI leg
 def run_fri(args):
     """FRI commit phase on a device-resident KoalaBear EF4 codeword of 2^23
@@ -615,7 +795,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving"], default="uneven-kb-2^30")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving"] + list(OPEN_WORKLOADS),
+                    default="uneven-kb-2^30")
     ap.add_argument("--requests", type=int, default=60, help="serving: number of requests")
     ap.add_argument("--load", type=float, default=0.8,
                     help="serving: offered load vs the plain form's one-at-a-time capacity")
@@ -629,6 +810,34 @@ def main():
     args = ap.parse_args()
 
     rank, world, local = dist_setup(args.gpus)
+    if args.workload in OPEN_WORKLOADS:
+        if args.impl == "reference":
+            if rank == 0:
+                ref = run_cpu_open(OPEN_WORKLOADS[args.workload](), 0, 1, 2, args.steps, args.warmup,
+                                   args.cpu_seconds)
+                print(json.dumps({
+                    "metric": OPEN_METRIC, "value": ref["value"], "unit": UNIT, "impl": "reference",
+                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": ref["seconds_per_run"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded uniform field elements",
+                    "config": {"workload": args.workload, "sample": ref["sample"]},
+                    "cpu_baseline": {"value": ref["value"], "unit": UNIT, "cores": ref["cores"], "kind": "port",
+                                     "sample": ref["sample"]},
+                    "e2e": {"value": ref["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                }), flush=True)
+            return
+        res = run_open(args, rank, world, local)
+        if rank == 0:
+            if not args.skip_cpu:
+                cpu = run_cpu_open(OPEN_WORKLOADS[args.workload](), 0, 1, 2, 1, 0, args.cpu_seconds)
+                res["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
+                                       "sample": cpu["sample"]}
+            print(json.dumps(res), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
     if args.workload in ("fri-kb-2^23", "serving"):
         if rank == 0:
             res = run_fri(args) if args.workload == "fri-kb-2^23" else run_serving(args)

@@ -11,14 +11,14 @@
 
 namespace pico {
 
-constexpr uint32_t kOpenMaxRows = 1024;  // low-coset rows per block of k_open_partial (log_rows <= 10)
+constexpr uint32_t kOpenMaxRows = 1024;  // low-coset rows whose weights k_open_partial holds in shared memory
 
 // One matrix of the opened-values pass and up to two of its points.
 struct OpenDesc {
   const uint32_t* lde;  // committed LDE, bit-reversed rows, row-major
   uint32_t w;
   uint32_t log_n;       // low coset (trace) height
-  uint32_t log_rows;    // rows per block
+  uint32_t log_rows;    // rows per block (at most log2(kOpenMaxRows) when w > 256)
   uint32_t n_pts;       // 1 or 2
   uint32_t pt[2];       // distinct-point index of each point (its 1/(z - x) table)
   uint32_t block0;      // first block of this descriptor
@@ -30,13 +30,20 @@ struct OpenDesc {
 // Reduced opening of one height.
 struct ReduceMat {
   const uint32_t* lde;
+  uint64_t magic;    // ceil(2^32 / w): f / w = (f * magic) >> 32 for f < 32 w, w <= 32
   uint32_t w;
-  uint32_t multi;    // 0: one point (slot, off); 1: n_terms (slot, off) terms from term0
+  uint32_t multi;    // 0: one point (slot, off); 1: n_terms terms from term0
   uint32_t slot, off;
   uint32_t n_terms, term0;
+  uint32_t vec;      // rows 16-byte aligned and w % 4 == 0: 16-byte loads
+  uint32_t pad;
 };
+// One (point, alpha^off) term of a matrix opened at several points: a = alpha^off
+// and W a (entries 1..3), Monty form.
 struct ReduceTerm {
   uint32_t slot, off;
+  uint32_t a[4];
+  uint32_t wa[4];
 };
 struct ReduceHeight {
   uint32_t log_h;
@@ -45,7 +52,9 @@ struct ReduceHeight {
   uint32_t accumulate;   // add to ro instead of overwriting
   const ReduceMat* mats;
   const ReduceTerm* terms;
-  const uint4* apow;     // alpha^k, EF4
+  const uint4* apow;     // alpha^k, EF4, k < apow_len
+  uint32_t apow_len;
+  uint32_t pad;
   const uint4* dinv[4];  // 1 / (z_slot - x_i)
   Ext4 K[4];             // sum over (m, z_slot) of alpha^off * sum_j alpha^j p_j(z)
   uint4* ro;
@@ -64,10 +73,14 @@ struct QuerySeg {
 
 cudaError_t launch_inv_denoms(int field, const uint32_t z[4], uint32_t log_h, TwiddleTables tw, uint32_t* out,
                               cudaStream_t st);
+// max_items: the largest n_pts * w of the descriptors (finalize grid width).
 cudaError_t launch_open_values(int field, const OpenDesc* descs, uint32_t n_desc, uint32_t n_blocks,
-                               const uint32_t* const* dinv_tables, TwiddleTables tw, uint32_t* partial,
-                               const uint32_t* scale, uint32_t* values, cudaStream_t st);
+                               uint32_t max_items, const uint32_t* const* dinv_tables, TwiddleTables tw,
+                               uint32_t* partial, const uint32_t* scale, uint32_t* values, cudaStream_t st);
 cudaError_t launch_reduce(int field, const ReduceHeight& h, cudaStream_t st);
+// Bounds guard of the reduction's tile copies (synchronous read-back / clear).
+cudaError_t open_guard_fetch(GuardRecord* dst);
+cudaError_t open_guard_clear();
 cudaError_t launch_gather_queries(const QuerySeg* segs, uint32_t n_segs, const uint32_t* indices, uint32_t n_queries,
                                   uint64_t query_words, uint32_t* out, cudaStream_t st);
 

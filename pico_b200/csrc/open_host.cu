@@ -218,7 +218,7 @@ struct Opening {
   pico_status enqueue_values(uint32_t* d_values) {
     std::vector<OpenDesc> descs;
     std::vector<Ext4> scale;
-    uint32_t blocks = 0;
+    uint32_t blocks = 0, max_items = 0;
     uint64_t part = 0;
     const uint32_t g = B::to_monty(F::GENERATOR);
     for (size_t i = 0; i < pairs.size();) {
@@ -234,7 +234,12 @@ struct Opening {
         d.lde = c->lde[a.m];
         d.w = w;
         d.log_n = c->log_N[a.m] - log_b;
-        d.log_rows = std::min<uint32_t>(d.log_n, 10);
+        // about 2^17 cells per block; at least kOpenMaxRows rows, and exactly
+        // that many for matrices wider than a block of threads
+        uint32_t lw = 0;
+        while ((1u << lw) < w) lw++;
+        d.log_rows = std::min<uint32_t>(d.log_n, w > 256 ? 10u : std::max<uint32_t>(10u, 17u - std::min(lw, 17u)));
+        max_items = std::max(max_items, np * w);
         d.n_pts = np;
         d.block0 = blocks;
         d.part_off = part;
@@ -266,7 +271,7 @@ struct Opening {
     if ((s = ar.upload(&d_descs, descs)) || (s = ar.upload(&d_scale, scale)) || (s = ar.upload(&d_dt, dtab)) ||
         (s = ar.get(&d_part, part * 16)))
       return s;
-    if ((s = cuda_status(launch_open_values(F::ID, d_descs, (uint32_t)descs.size(), blocks, d_dt,
+    if ((s = cuda_status(launch_open_values(F::ID, d_descs, (uint32_t)descs.size(), blocks, max_items, d_dt,
                                             twiddles(ctx, F::ID), (uint32_t*)d_part, (const uint32_t*)d_scale,
                                             d_values, st),
                          "opened values")))
@@ -356,6 +361,7 @@ struct Opening {
         L.h.n_slots = (uint32_t)ns;
         L.h.accumulate = s0 > 0;
         L.h.apow = reinterpret_cast<const uint4*>(d_apow);
+        L.h.apow_len = (uint32_t)T;
         L.h.ro = reinterpret_cast<uint4*>(p);
         for (size_t q = 0; q < ns; q++) {
           L.h.dinv[q] = reinterpret_cast<const uint4*>(dtab[slots[s0 + q]]);
@@ -375,7 +381,16 @@ struct Opening {
               auto it = std::find(slots.begin() + s0, slots.begin() + s0 + ns, pairs[k].pt);
               if (it == slots.begin() + s0 + ns) continue;
               const uint32_t sl = (uint32_t)(it - (slots.begin() + s0));
-              terms.push_back(ReduceTerm{sl, off[k]});
+              ReduceTerm T;
+              memset(&T, 0, sizeof T);
+              T.slot = sl;
+              T.off = off[k];
+              constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
+              for (int l = 0; l < 4; l++) {
+                T.a[l] = apow[off[k]].c[l];
+                T.wa[l] = l ? B::mul(T.a[l], Wm) : 0u;
+              }
+              terms.push_back(T);
               L.h.K[sl] = E::add(L.h.K[sl], E::mul(apow[off[k]], rys[k]));
             }
             if (!terms.empty()) {
@@ -383,6 +398,8 @@ struct Opening {
               memset(&R, 0, sizeof R);
               R.lde = c->lde[a.m];
               R.w = c->width[a.m];
+              R.magic = ((1ull << 32) + R.w - 1) / R.w;
+              R.vec = (R.w % 4 == 0 && ((uintptr_t)R.lde & 15) == 0) ? 1u : 0u;
               if (terms.size() == 1) {
                 R.multi = 0;
                 R.slot = terms[0].slot;
@@ -437,6 +454,17 @@ struct EventTimer {
   }
 };
 
+pico_status open_guard_verdict() {
+  GuardRecord g{};
+  pico_status s = cuda_status(open_guard_fetch(&g), "guard read-back");
+  if (s || !g.count) return s;
+  set_error("internal bounds guard: reduction tile copies skipped %llu access(es); first: tag %llu, tile word %llu, "
+            "matrix word %llu, block %llu, thread %llu",
+            g.count, g.tag, g.offset, g.extent, g.block, g.thread);
+  open_guard_clear();
+  return PICO_ERR_CUDA;
+}
+
 template <class F>
 pico_status pcs_open_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_t n_batches, const Shape& sh,
                        const pico_fri_params* fp, pico_challenger* ch, uint32_t* values, uint32_t* commit_roots,
@@ -485,6 +513,7 @@ pico_status pcs_open_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_t n
     if ((s = tm.mark(O.st))) return s;
     if ((s = O.enqueue_reduce(values, alpha, 32, ro, &reduce_cells))) return s;
     if ((s = tm.mark(O.st))) return s;
+    if ((s = cuda_status(cudaStreamSynchronize(O.st), "reduced openings"))) return s;
     std::vector<uint32_t*> cws(R + 1), trees(R);
     std::vector<const uint32_t*> inject(R, nullptr);
     cws[0] = ro[log_max];
@@ -621,9 +650,10 @@ pico_status pcs_open_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_t n
   };
   pico_status s = run();
   if (!s) s = guard_enqueue(ctx, O.slot, O.st);
-  pico_status s2 = cuda_status(cudaStreamSynchronize(O.st), "pcs_open");
-  if (!s) s = s2;
+  const cudaError_t e = cudaStreamSynchronize(O.st);
+  if (!s) s = cuda_status(e, "pcs_open");  // an earlier failure keeps its own message
   if (!s) s = guard_verdict(ctx, O.slot);
+  if (!s) s = open_guard_verdict();
   if (!s) *ch = tr;
   if (!s && stats) {
     memset(stats, 0, sizeof *stats);
@@ -662,8 +692,8 @@ pico_status open_values_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_
     return PICO_OK;
   };
   pico_status s = run();
-  pico_status s2 = cuda_status(cudaStreamSynchronize(O.st), "open_values");
-  if (!s) s = s2;
+  const cudaError_t e = cudaStreamSynchronize(O.st);
+  if (!s) s = cuda_status(e, "open_values");
   O.end();
   return s;
 }
@@ -690,8 +720,9 @@ pico_status reduced_opening_t(pico_ctx* ctx, const pico_open_batch* batches, uin
                        "reduced opening");
   };
   pico_status s = run();
-  pico_status s2 = cuda_status(cudaStreamSynchronize(O.st), "reduced_opening");
-  if (!s) s = s2;
+  const cudaError_t e = cudaStreamSynchronize(O.st);
+  if (!s) s = cuda_status(e, "reduced_opening");
+  if (!s) s = open_guard_verdict();
   O.end();
   return s;
 }

@@ -34,39 +34,24 @@ struct Lazy {
       ((unsigned __int128)1 << 64);
   static_assert(kFourFit, "four products after a fold must fit 64 bits");
   static_assert(((C + 1) << 32) < ((uint64_t)F::P << 32), "a folded sum must be reducible by REDC");
-  static __device__ __forceinline__ uint64_t fold(uint64_t x) { return (x >> 32) * C + (uint32_t)x; }
+  // acc += a * b (one 32x32 -> 64-bit multiply-add)
+  static __device__ __forceinline__ void mac(uint64_t& acc, uint32_t a, uint32_t b) {
+    asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc) : "r"(a), "r"(b));
+  }
+  // hi * C + lo: congruent mod p, below 2^32 (C + 1)
+  static __device__ __forceinline__ uint64_t fold(uint64_t x) {
+    uint32_t lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(x));
+    uint64_t r;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(hi), "n"((uint32_t)C), "l"((uint64_t)lo));
+    return r;
+  }
   static __device__ __forceinline__ uint32_t finish(uint64_t x) { return Fp<F>::canon(Fp<F>::redc(fold(x))); }
 };
 
 template <class F>
 __device__ __forceinline__ uint32_t ompow(const TwiddleTables& tw, uint32_t E) {
   return Fp<F>::mul(__ldg(tw.hi + (E >> 14)), __ldg(tw.lo + (E & 0x3fffu)));
-}
-
-// Inverse through the quadratic subfield F[Y], Y = X^2 (Y^2 = W): with
-// a = e + X o, a * (e - X o) = e^2 - Y o^2 =: b in F[Y], and b^-1 = conj(b) / N(b).
-template <class F>
-__device__ __forceinline__ Ext4 ef_inv(const Ext4& a) {
-  using B = Fp<F>;
-  constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
-  const uint32_t a0 = a.c[0], a1 = a.c[1], a2 = a.c[2], a3 = a.c[3];
-  // e^2 = (a0^2 + W a2^2) + 2 a0 a2 Y ; o^2 = (a1^2 + W a3^2) + 2 a1 a3 Y
-  const uint32_t e0 = B::add(B::mul(a0, a0), B::mul(Wm, B::mul(a2, a2)));
-  const uint32_t e1 = B::dbl(B::mul(a0, a2));
-  const uint32_t o0 = B::add(B::mul(a1, a1), B::mul(Wm, B::mul(a3, a3)));
-  const uint32_t o1 = B::dbl(B::mul(a1, a3));
-  // b = e^2 - Y o^2 = (e0 - W o1) + (e1 - o0) Y
-  const uint32_t b0 = B::sub(e0, B::mul(Wm, o1));
-  const uint32_t b1 = B::sub(e1, o0);
-  const uint32_t nrm = B::sub(B::mul(b0, b0), B::mul(Wm, B::mul(b1, b1)));
-  const uint32_t ni = B::inv(nrm);
-  const uint32_t c = B::mul(b0, ni), d = B::neg(B::mul(b1, ni));  // b^-1 = c + d Y
-  Ext4 r;
-  r.c[0] = B::add(B::mul(a0, c), B::mul(Wm, B::mul(a2, d)));
-  r.c[1] = B::neg(B::add(B::mul(a1, c), B::mul(Wm, B::mul(a3, d))));
-  r.c[2] = B::add(B::mul(a0, d), B::mul(a2, c));
-  r.c[3] = B::neg(B::add(B::mul(a1, d), B::mul(a3, c)));
-  return r;
 }
 
 __device__ __forceinline__ Ext4 ld4(const uint4* p) {
@@ -76,21 +61,63 @@ __device__ __forceinline__ Ext4 ld4(const uint4* p) {
 __device__ __forceinline__ uint4 st4(const Ext4& a) { return make_uint4(a.c[0], a.c[1], a.c[2], a.c[3]); }
 
 // ---------------------------------------------------------------------------
+// 1/(z - x_i) for eight consecutive rows per thread.  Each inverse goes through
+// the quadratic subfield F[Y], Y = X^2 (Y^2 = W): with a = e + X o,
+// a (e - X o) = e^2 - Y o^2 =: b in F[Y] and b^-1 = conj(b) / N(b), N(b) in F.
+// The eight norms share one base-field inversion (Montgomery's simultaneous
+// inversion: prefix products, one inverse, back-substitution).
+constexpr uint32_t kInvPerThread = 8;
+
 template <class F>
-__global__ void k_inv_denoms(Ext4 z, uint32_t log_h, uint32_t g_monty, TwiddleTables tw, uint4* out) {
-  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= (1ull << log_h)) return;
-  const uint32_t E = (uint32_t)bitrev64(i, (int)log_h) << (F::TWO_ADICITY - log_h);
-  const uint32_t x = Fp<F>::mul(g_monty, ompow<F>(tw, E));
-  Ext4 d = z;
-  d.c[0] = Fp<F>::sub(d.c[0], x);
-  out[i] = st4(ef_inv<F>(d));
+__global__ void __launch_bounds__(256) k_inv_denoms(Ext4 z, uint32_t log_h, uint32_t g_monty, TwiddleTables tw,
+                                                    uint4* out) {
+  using B = Fp<F>;
+  constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
+  const uint64_t n = 1ull << log_h;
+  const uint64_t i0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) * kInvPerThread;
+  if (i0 >= n) return;
+  const uint32_t cnt = n - i0 < kInvPerThread ? (uint32_t)(n - i0) : kInvPerThread;
+  uint32_t b0[kInvPerThread], b1[kInvPerThread], nrm[kInvPerThread], pre[kInvPerThread];
+  Ext4 a[kInvPerThread];
+  uint32_t run = F::ONE;
+#pragma unroll
+  for (uint32_t k = 0; k < kInvPerThread; k++) {
+    const uint64_t i = i0 + (k < cnt ? k : 0);
+    const uint32_t E = (uint32_t)bitrev64(i, (int)log_h) << (F::TWO_ADICITY - log_h);
+    a[k] = z;
+    a[k].c[0] = B::sub(z.c[0], B::mul(g_monty, ompow<F>(tw, E)));
+    const uint32_t x0 = a[k].c[0], x1 = a[k].c[1], x2 = a[k].c[2], x3 = a[k].c[3];
+    const uint32_t e0 = B::add(B::mul(x0, x0), B::mul(Wm, B::mul(x2, x2)));
+    const uint32_t e1 = B::dbl(B::mul(x0, x2));
+    const uint32_t o0 = B::add(B::mul(x1, x1), B::mul(Wm, B::mul(x3, x3)));
+    const uint32_t o1 = B::dbl(B::mul(x1, x3));
+    b0[k] = B::sub(e0, B::mul(Wm, o1));
+    b1[k] = B::sub(e1, o0);
+    nrm[k] = B::sub(B::mul(b0[k], b0[k]), B::mul(Wm, B::mul(b1[k], b1[k])));
+    pre[k] = run;  // product of the norms before k
+    run = B::mul(run, nrm[k]);
+  }
+  uint32_t inv = B::inv(run);
+#pragma unroll
+  for (int k = kInvPerThread - 1; k >= 0; k--) {
+    const uint32_t ni = B::mul(inv, pre[k]);  // 1 / nrm[k]
+    inv = B::mul(inv, nrm[k]);
+    const uint32_t c = B::mul(b0[k], ni), d = B::neg(B::mul(b1[k], ni));
+    const uint32_t x0 = a[k].c[0], x1 = a[k].c[1], x2 = a[k].c[2], x3 = a[k].c[3];
+    Ext4 r;
+    r.c[0] = B::add(B::mul(x0, c), B::mul(Wm, B::mul(x2, d)));
+    r.c[1] = B::neg(B::add(B::mul(x1, c), B::mul(Wm, B::mul(x3, d))));
+    r.c[2] = B::add(B::mul(x0, d), B::mul(x2, c));
+    r.c[3] = B::neg(B::add(B::mul(x1, d), B::mul(x3, c)));
+    if ((uint32_t)k < cnt) out[i0 + k] = st4(r);
+  }
 }
 
 cudaError_t launch_inv_denoms(int field, const uint32_t z[4], uint32_t log_h, TwiddleTables tw, uint32_t* out,
                               cudaStream_t st) {
   const uint64_t n = 1ull << log_h;
-  const unsigned blocks = (unsigned)((n + 255) / 256);
+  const uint64_t threads = (n + kInvPerThread - 1) / kInvPerThread;
+  const unsigned blocks = (unsigned)((threads + 255) / 256);
   Ext4 e{{z[0], z[1], z[2], z[3]}};
   if (field == 0)
     k_inv_denoms<KoalaBear><<<blocks, 256, 0, st>>>(e, log_h, Fp<KoalaBear>::to_monty(KoalaBear::GENERATOR), tw,
@@ -112,84 +139,106 @@ constexpr int kOpenThreads = 256;
 template <class F, int NP>
 __device__ void open_block(const OpenDesc& d, uint32_t chunk, const TwiddleTables& tw, const uint4* const* dinv,
                            uint4* partial, Ext4 (*coef)[2], uint32_t (*red)[2][4]) {
-  const uint32_t R = 1u << d.log_rows;
+  const uint32_t R = 1u << d.log_rows;  // rows of this block; above kOpenMaxRows only when w <= kOpenThreads
   const uint64_t r0 = (uint64_t)chunk << d.log_rows;
   const uint32_t t = threadIdx.x;
-  for (uint32_t r = t; r < R; r += kOpenThreads) {
-    const uint64_t i = r0 + r;
-    const uint32_t E = (uint32_t)bitrev64(i, (int)d.log_n) << (F::TWO_ADICITY - d.log_n);
-    const uint32_t wk = ompow<F>(tw, E);
-#pragma unroll
-    for (int p = 0; p < NP; p++) coef[r][p] = Ef<F>::scale(ld4(dinv[p] + i), wk);
-  }
-  __syncthreads();
   const uint32_t w = d.w;
-  const uint32_t* base = d.lde + r0 * w;
-  if (w <= (uint32_t)kOpenThreads) {
-    const uint32_t rpp = kOpenThreads / w;  // rows per pass
-    const uint32_t ri = t / w, j = t - ri * w;
-    uint64_t acc[NP][4] = {};
-    if (ri < rpp) {
-      uint32_t k = 0;
-      for (uint32_t r = ri; r < R; r += rpp, k++) {
-        const uint32_t y = __ldg(base + (uint64_t)r * w + j);
+  const bool narrow = w <= (uint32_t)kOpenThreads;
+  const uint32_t rpp = narrow ? kOpenThreads / w : 1;  // rows per pass (narrow form)
+  const uint32_t ri = narrow ? t / w : 0, j = narrow ? t - ri * w : t;
+  uint64_t acc[NP][4] = {};
+  for (uint32_t sub = 0; sub < R; sub += kOpenMaxRows) {
+    const uint32_t Rs = min(R - sub, kOpenMaxRows);
+    for (uint32_t r = t; r < Rs; r += kOpenThreads) {
+      const uint64_t i = r0 + sub + r;
+      const uint32_t E = (uint32_t)bitrev64(i, (int)d.log_n) << (F::TWO_ADICITY - d.log_n);
+      const uint32_t wk = ompow<F>(tw, E);
 #pragma unroll
-        for (int p = 0; p < NP; p++)
-#pragma unroll
-          for (int l = 0; l < 4; l++) acc[p][l] += (uint64_t)coef[r][p].c[l] * y;
-        if ((k & 3) == 3) {
-#pragma unroll
-          for (int p = 0; p < NP; p++)
-#pragma unroll
-            for (int l = 0; l < 4; l++) acc[p][l] = Lazy<F>::fold(acc[p][l]);
-        }
-      }
+      for (int p = 0; p < NP; p++) coef[r][p] = Ef<F>::scale(ld4(dinv[p] + i), wk);
     }
-#pragma unroll
-    for (int p = 0; p < NP; p++)
-#pragma unroll
-      for (int l = 0; l < 4; l++) red[t][p][l] = ri < rpp ? Lazy<F>::finish(acc[p][l]) : 0u;
     __syncthreads();
-    if (t < w) {
+    const uint32_t* base = d.lde + (r0 + sub) * w;
+    if (narrow) {
+      if (ri < rpp) {
+        // eight rows per batch, their loads issued together
+        for (uint32_t r = ri; r < Rs; r += 8 * rpp) {
+          uint32_t y[8];
 #pragma unroll
-      for (int p = 0; p < NP; p++) {
-        Ext4 s{{0, 0, 0, 0}};
-        for (uint32_t q = 0; q < rpp; q++) {
-          const uint32_t* v = red[q * w + t][p];
-          s = Ef<F>::add(s, Ext4{{v[0], v[1], v[2], v[3]}});
+          for (int u = 0; u < 8; u++) {
+            const uint32_t rr = r + u * rpp;
+            y[u] = rr < Rs ? __ldg(base + (uint64_t)rr * w + j) : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const uint32_t rr = min(r + u * rpp, Rs - 1);  // past the end: y = 0 adds nothing
+#pragma unroll
+            for (int p = 0; p < NP; p++)
+#pragma unroll
+              for (int l = 0; l < 4; l++) Lazy<F>::mac(acc[p][l], coef[rr][p].c[l], y[u]);
+            if ((u & 3) == 3) {
+#pragma unroll
+              for (int p = 0; p < NP; p++)
+#pragma unroll
+                for (int l = 0; l < 4; l++) acc[p][l] = Lazy<F>::fold(acc[p][l]);
+            }
+          }
         }
-        partial[d.part_off + ((uint64_t)chunk * NP + p) * w + t] = st4(s);
+      }
+    } else {
+      // wide: one sub-chunk only (R <= kOpenMaxRows), column tiles of kOpenThreads
+      for (uint32_t jj = t; jj < w; jj += kOpenThreads) {
+        uint64_t a2[NP][4] = {};
+        for (uint32_t r = 0; r < Rs; r += 8) {
+          uint32_t y[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) y[u] = r + u < Rs ? __ldg(base + (uint64_t)(r + u) * w + jj) : 0u;
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const uint32_t rr = min(r + u, Rs - 1);
+#pragma unroll
+            for (int p = 0; p < NP; p++)
+#pragma unroll
+              for (int l = 0; l < 4; l++) Lazy<F>::mac(a2[p][l], coef[rr][p].c[l], y[u]);
+            if ((u & 3) == 3) {
+#pragma unroll
+              for (int p = 0; p < NP; p++)
+#pragma unroll
+                for (int l = 0; l < 4; l++) a2[p][l] = Lazy<F>::fold(a2[p][l]);
+            }
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+          Ext4 s;
+#pragma unroll
+          for (int l = 0; l < 4; l++) s.c[l] = Lazy<F>::finish(a2[p][l]);
+          partial[d.part_off + ((uint64_t)chunk * NP + p) * w + jj] = st4(s);
+        }
       }
     }
-  } else {
-    for (uint32_t j = t; j < w; j += kOpenThreads) {
-      uint64_t acc[NP][4] = {};
-      for (uint32_t r = 0; r < R; r++) {
-        const uint32_t y = __ldg(base + (uint64_t)r * w + j);
+    __syncthreads();
+  }
+  if (!narrow) return;
 #pragma unroll
-        for (int p = 0; p < NP; p++)
+  for (int p = 0; p < NP; p++)
 #pragma unroll
-          for (int l = 0; l < 4; l++) acc[p][l] += (uint64_t)coef[r][p].c[l] * y;
-        if ((r & 3) == 3) {
+    for (int l = 0; l < 4; l++) red[t][p][l] = ri < rpp ? Lazy<F>::finish(acc[p][l]) : 0u;
+  __syncthreads();
+  if (t < w) {
 #pragma unroll
-          for (int p = 0; p < NP; p++)
-#pragma unroll
-            for (int l = 0; l < 4; l++) acc[p][l] = Lazy<F>::fold(acc[p][l]);
-        }
+    for (int p = 0; p < NP; p++) {
+      Ext4 s{{0, 0, 0, 0}};
+      for (uint32_t q = 0; q < rpp; q++) {
+        const uint32_t* v = red[q * w + t][p];
+        s = Ef<F>::add(s, Ext4{{v[0], v[1], v[2], v[3]}});
       }
-#pragma unroll
-      for (int p = 0; p < NP; p++) {
-        Ext4 s;
-#pragma unroll
-        for (int l = 0; l < 4; l++) s.c[l] = Lazy<F>::finish(acc[p][l]);
-        partial[d.part_off + ((uint64_t)chunk * NP + p) * w + j] = st4(s);
-      }
+      partial[d.part_off + ((uint64_t)chunk * NP + p) * w + t] = st4(s);
     }
   }
 }
 
 template <class F>
-__global__ void __launch_bounds__(kOpenThreads) k_open_partial(const OpenDesc* descs, uint32_t n_desc,
+__global__ void __launch_bounds__(kOpenThreads, 3) k_open_partial(const OpenDesc* descs, uint32_t n_desc,
                                                                const uint4* const* dinv_tables, TwiddleTables tw,
                                                                uint4* partial) {
   __shared__ Ext4 coef[kOpenMaxRows][2];
@@ -211,126 +260,295 @@ __global__ void __launch_bounds__(kOpenThreads) k_open_partial(const OpenDesc* d
     open_block<F, 1>(d, chunk, tw, dinv, partial, coef, red);
 }
 
+// One warp per output value: the lanes stride over the blocks' partial sums,
+// then a shuffle tree adds the 32 lane sums.
 template <class F>
 __global__ void k_open_finalize(const OpenDesc* descs, const uint4* partial, const Ext4* scale, uint4* values) {
-  const OpenDesc d = descs[blockIdx.x];
-  const uint32_t chunks = 1u << (d.log_n - d.log_rows);
-  for (uint32_t item = threadIdx.x; item < d.n_pts * d.w; item += blockDim.x) {
-    const uint32_t p = item / d.w, j = item - p * d.w;
-    Ext4 s{{0, 0, 0, 0}};
-    for (uint32_t c = 0; c < chunks; c++) s = Ef<F>::add(s, ld4(partial + d.part_off + ((uint64_t)c * d.n_pts + p) * d.w + j));
-    values[d.out_off[p] + j] = st4(Ef<F>::mul(s, scale[2 * blockIdx.x + p]));
+  const OpenDesc* d = descs + blockIdx.y;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t n_pts = d->n_pts, w = d->w;
+  if (item >= n_pts * w) return;
+  const uint32_t chunks = 1u << (d->log_n - d->log_rows);
+  const uint32_t p = item / w, j = item - p * w;
+  const uint4* src = partial + d->part_off + (uint64_t)p * w + j;
+  const uint64_t stride = (uint64_t)n_pts * w;
+  Ext4 s{{0, 0, 0, 0}};
+  for (uint32_t c = lane; c < chunks; c += 32) s = Ef<F>::add(s, ld4(src + c * stride));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Ext4 t;
+#pragma unroll
+    for (int l = 0; l < 4; l++) t.c[l] = __shfl_xor_sync(0xffffffffu, s.c[l], o);
+    s = Ef<F>::add(s, t);
   }
+  if (lane == 0) values[d->out_off[p] + j] = st4(Ef<F>::mul(s, scale[2 * blockIdx.y + p]));
 }
 
 cudaError_t launch_open_values(int field, const OpenDesc* descs, uint32_t n_desc, uint32_t n_blocks,
-                               const uint32_t* const* dinv_tables, TwiddleTables tw, uint32_t* partial,
-                               const uint32_t* scale, uint32_t* values, cudaStream_t st) {
+                               uint32_t max_items, const uint32_t* const* dinv_tables, TwiddleTables tw,
+                               uint32_t* partial, const uint32_t* scale, uint32_t* values, cudaStream_t st) {
   if (n_desc == 0) return cudaSuccess;
+  const unsigned fin_tiles = (max_items + 7) / 8;  // eight warps (values) per block
   auto dt = reinterpret_cast<const uint4* const*>(dinv_tables);
   auto pa = reinterpret_cast<uint4*>(partial);
   auto sc = reinterpret_cast<const Ext4*>(scale);
   auto va = reinterpret_cast<uint4*>(values);
   if (field == 0) {
     k_open_partial<KoalaBear><<<n_blocks, kOpenThreads, 0, st>>>(descs, n_desc, dt, tw, pa);
-    k_open_finalize<KoalaBear><<<n_desc, 256, 0, st>>>(descs, pa, sc, va);
+    k_open_finalize<KoalaBear><<<dim3(fin_tiles, n_desc), 256, 0, st>>>(descs, pa, sc, va);
   } else {
     k_open_partial<BabyBear><<<n_blocks, kOpenThreads, 0, st>>>(descs, n_desc, dt, tw, pa);
-    k_open_finalize<BabyBear><<<n_desc, 256, 0, st>>>(descs, pa, sc, va);
+    k_open_finalize<BabyBear><<<dim3(fin_tiles, n_desc), 256, 0, st>>>(descs, pa, sc, va);
   }
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// Reduced opening of one height: one thread per row.
+// Reduced opening of one height.  Lane l of a warp owns row row0 + l; the
+// warp stages its 32 rows through shared memory in tiles of 32 columns, loaded
+// with coalesced reads (a matrix of at most 32 columns as one contiguous block
+// of 32 rows), and each lane reads its row back across the banks (row stride
+// 33 words).  The alpha powers are read by all lanes at the same address.
+constexpr int kReduceWarps = 4;
+constexpr int kTileStride = 36;  // words per tile row: 16-byte aligned; eight lanes' 16-byte reads cover the 32 banks
+constexpr int kTileWords = 32 * kTileStride;        // data part of a tile buffer
+constexpr int kTileBufWords = kTileWords + 32 * 4;   // + the 32 alpha powers of its columns
+
+template <class F>
+__device__ __forceinline__ void mac4(uint64_t t[4], const uint4& c, uint32_t y) {
+  Lazy<F>::mac(t[0], c.x, y);
+  Lazy<F>::mac(t[1], c.y, y);
+  Lazy<F>::mac(t[2], c.z, y);
+  Lazy<F>::mac(t[3], c.w, y);
+}
+
+// t += sum_j coef[j] * row[j] over one tile row of cw columns (t folded on return)
+template <class F>
+__device__ __forceinline__ void lazy_row_tile(uint64_t t[4], const uint32_t* tile_row, const uint4* coef, uint32_t cw) {
+  uint32_t j = 0;
+  for (; j + 4 <= cw; j += 4) {
+    const uint4 y = *reinterpret_cast<const uint4*>(tile_row + j);
+    mac4<F>(t, coef[j], y.x);
+    mac4<F>(t, coef[j + 1], y.y);
+    mac4<F>(t, coef[j + 2], y.z);
+    mac4<F>(t, coef[j + 3], y.w);
+#pragma unroll
+    for (int l = 0; l < 4; l++) t[l] = Lazy<F>::fold(t[l]);
+  }
+  for (; j < cw; j++) mac4<F>(t, coef[j], tile_row[j]);
+#pragma unroll
+  for (int l = 0; l < 4; l++) t[l] = Lazy<F>::fold(t[l]);
+}
+
+// acc (folded) += a * b in EF4, a given with W*a1..W*a3 (four products per limb)
+template <class F>
+__device__ __forceinline__ void lazy_ef_mac(uint64_t acc[4], const uint32_t a[4], const uint32_t wa[4], const Ext4& b) {
+  using L = Lazy<F>;
+#pragma unroll
+  for (int l = 0; l < 4; l++) acc[l] = L::fold(acc[l]);
+  L::mac(acc[0], a[0], b.c[0]); L::mac(acc[0], wa[1], b.c[3]); L::mac(acc[0], wa[2], b.c[2]); L::mac(acc[0], wa[3], b.c[1]);
+  L::mac(acc[1], a[0], b.c[1]); L::mac(acc[1], a[1], b.c[0]); L::mac(acc[1], wa[2], b.c[3]); L::mac(acc[1], wa[3], b.c[2]);
+  L::mac(acc[2], a[0], b.c[2]); L::mac(acc[2], a[1], b.c[1]); L::mac(acc[2], a[2], b.c[0]); L::mac(acc[2], wa[3], b.c[3]);
+  L::mac(acc[3], a[0], b.c[3]); L::mac(acc[3], a[1], b.c[2]); L::mac(acc[3], a[2], b.c[1]); L::mac(acc[3], a[3], b.c[0]);
+}
+
+// Bounds guard of the tile copies: a copy whose shared-memory slot or source
+// row/column falls outside its tile or matrix (or a 16-byte copy that is not
+// 16-byte aligned) is skipped and the first one recorded; the entry points
+// report it after their final synchronisation.
+__device__ GuardRecord g_open_guard;
+__device__ __noinline__ void open_guard_trip(unsigned long long tag, unsigned long long offset,
+                                             unsigned long long extent) {
+  if (atomicAdd(&g_open_guard.count, 1ull) == 0) {
+    g_open_guard.tag = tag;
+    g_open_guard.offset = offset;
+    g_open_guard.extent = extent;
+    g_open_guard.block = blockIdx.x;
+    g_open_guard.thread = threadIdx.x;
+  }
+}
+
+cudaError_t open_guard_fetch(GuardRecord* dst) { return cudaMemcpyFromSymbol(dst, g_open_guard, sizeof(GuardRecord)); }
+cudaError_t open_guard_clear() {
+  GuardRecord z{};
+  return cudaMemcpyToSymbol(g_open_guard, &z, sizeof z);
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(uint32_t* dst, const uint32_t* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Copy tile j0 of matrix M (rows row0 .. row0 + rows - 1, columns j0 .. j0 + 31)
+// into `tile` with asynchronous copies; a matrix of at most 32 columns is one
+// tile taken as its rows * w contiguous words.
+__device__ __forceinline__ void issue_tile(const ReduceMat& M, const uint4* apow, uint32_t apow_len, uint64_t N,
+                                           uint64_t row0, uint32_t rows, uint32_t j0, uint32_t* tile, uint32_t lane) {
+  const uint32_t w = M.w;
+  {
+    // the tile's alpha powers: alpha^(off + j0 + lane) (one point) or alpha^(j0 + lane)
+    const uint32_t cw = w <= 32 ? w : min(32u, w - j0);
+    const uint32_t k = (M.multi ? 0u : M.off) + j0 + lane;
+    if (lane < cw) {
+      if (k < apow_len)
+        cp_async16(tile + kTileWords + 4 * lane, reinterpret_cast<const uint32_t*>(apow + k));
+      else
+        open_guard_trip(kGuardTwiddle, k, apow_len);
+    }
+  }
+  const uint32_t* src = M.lde + row0 * w;
+  const uint64_t limit = N * w;  // words of the matrix
+  // checked copy: word `so` of the matrix (from src) to word `dofs` of the tile
+  auto copy = [&](uint32_t dofs, uint64_t so, uint32_t words) {
+    const uint64_t g = row0 * w + so;
+    if (dofs + words > (uint32_t)kTileWords || g + words > limit) {
+      open_guard_trip(kGuardTile, dofs, g);
+      return;
+    }
+    if (words == 4) {
+      if ((((uintptr_t)(tile + dofs)) | ((uintptr_t)(src + so))) & 15u) {
+        open_guard_trip(kGuardLoad, dofs, g);
+        return;
+      }
+      cp_async16(tile + dofs, src + so);
+    } else {
+      cp_async4(tile + dofs, src + so);
+    }
+  };
+  if (w <= 32) {
+    const uint32_t total = rows * w;
+    if (M.vec) {
+      for (uint32_t f = 4 * lane; f < total; f += 4 * 32) {
+        const uint32_t r = (uint32_t)(((uint64_t)f * M.magic) >> 32);  // f / w
+        copy(r * kTileStride + (f - r * w), f, 4);
+      }
+    } else {
+      for (uint32_t f = lane; f < total; f += 32) {
+        const uint32_t r = (uint32_t)(((uint64_t)f * M.magic) >> 32);
+        copy(r * kTileStride + (f - r * w), f, 1);
+      }
+    }
+    return;
+  }
+  const uint32_t cw = min(32u, w - j0);
+  if (M.vec) {
+    // eight lanes per row, four rows per step; cw is a multiple of 4
+    const uint32_t rr = lane >> 3, q = (lane & 7) * 4;
+    if (q < cw)
+      for (uint32_t r = rr; r < rows; r += 4) copy(r * kTileStride + q, (uint64_t)r * w + j0 + q, 4);
+  } else if (lane < cw) {
+    for (uint32_t r = 0; r < rows; r++) copy(r * kTileStride + lane, (uint64_t)r * w + j0 + lane, 1);
+  }
+}
+
+// Lane l of a warp owns row row0 + l.  The warp walks the tiles of all
+// matrices of the height (32 rows x 32 columns; one tile for a matrix of at
+// most 32 columns), double-buffered: the copy of the next tile is in flight
+// while the current one is reduced.  Each lane reads its row back across the
+// banks; the alpha powers are read by all lanes at the same address.
 template <class F, int NS>
-__global__ void __launch_bounds__(256) k_reduce(ReduceHeight h) {
+__global__ void __launch_bounds__(32 * kReduceWarps, 5) k_reduce(ReduceHeight h) {
+  using B = Fp<F>;
   using E = Ef<F>;
   using L = Lazy<F>;
-  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= (1ull << h.log_h)) return;
+  constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
+  __shared__ __align__(16) uint32_t tiles[kReduceWarps][2][kTileBufWords];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t N = 1ull << h.log_h;
+  const uint64_t row0 = (blockIdx.x * (uint64_t)kReduceWarps + warp) * 32;
+  if (row0 >= N || h.n_mats == 0) return;  // whole warp beyond the height
+  const uint32_t rows = N - row0 < 32 ? (uint32_t)(N - row0) : 32u;
+  const uint64_t i = row0 + lane;
   uint64_t acc[NS][4] = {};
-  for (uint32_t m = 0; m < h.n_mats; m++) {
-    const ReduceMat M = h.mats[m];
-    const uint32_t* row = M.lde + i * M.w;
-    const uint4* coef = h.apow + (M.multi ? 0u : M.off);
-    uint64_t t[4] = {0, 0, 0, 0};
-    uint32_t j = 0;
-    for (; j + 4 <= M.w; j += 4) {
+  uint64_t t[4] = {0, 0, 0, 0};
+  uint32_t m = 0, j0 = 0, buf = 0;
+  ReduceMat M = h.mats[0];
+  issue_tile(M, h.apow, h.apow_len, N, row0, rows, 0, tiles[warp][0], lane);
+  cp_async_commit();
+  for (;;) {
+    // the tile after (m, j0)
+    uint32_t m2 = m, j2 = j0 + 32;
+    if (M.w <= 32 || j2 >= M.w) {
+      m2 = m + 1;
+      j2 = 0;
+    }
+    ReduceMat M2;
+    if (m2 < h.n_mats) {
+      M2 = h.mats[m2];
+      issue_tile(M2, h.apow, h.apow_len, N, row0, rows, j2, tiles[warp][buf ^ 1], lane);
+    }
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncwarp();
+    const uint32_t cw = M.w <= 32 ? M.w : min(32u, M.w - j0);
+    const uint4* coef = reinterpret_cast<const uint4*>(tiles[warp][buf] + kTileWords);
+    lazy_row_tile<F>(t, tiles[warp][buf] + lane * kTileStride, coef, cw);
+    __syncwarp();  // the buffer is refilled next iteration
+    if (m2 != m) {
+      // matrix m done
+      if (!M.multi) {
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const uint32_t y = __ldg(row + j + u);
-        const uint4 c = __ldg(coef + j + u);
-        t[0] += (uint64_t)c.x * y;
-        t[1] += (uint64_t)c.y * y;
-        t[2] += (uint64_t)c.z * y;
-        t[3] += (uint64_t)c.w * y;
+        for (int q = 0; q < NS; q++)
+          if (q == (int)M.slot) {
+#pragma unroll
+            for (int l = 0; l < 4; l++) acc[q][l] = L::fold(L::fold(acc[q][l]) + t[l]);
+          }
+      } else {
+        // r = sum_j alpha^j M[i][j]; each (slot, alpha^off) term adds alpha^off * r
+        Ext4 r;
+#pragma unroll
+        for (int l = 0; l < 4; l++) r.c[l] = L::finish(t[l]);
+        for (uint32_t k = 0; k < M.n_terms; k++) {
+          const ReduceTerm T = h.terms[M.term0 + k];
+#pragma unroll
+          for (int q = 0; q < NS; q++)
+            if (q == (int)T.slot) lazy_ef_mac<F>(acc[q], T.a, T.wa, r);
+        }
       }
 #pragma unroll
-      for (int l = 0; l < 4; l++) t[l] = L::fold(t[l]);
+      for (int l = 0; l < 4; l++) t[l] = 0;
+      if (m2 >= h.n_mats) break;
+      M = M2;
     }
-    for (; j < M.w; j++) {
-      const uint32_t y = __ldg(row + j);
-      const uint4 c = __ldg(coef + j);
-      t[0] += (uint64_t)c.x * y;
-      t[1] += (uint64_t)c.y * y;
-      t[2] += (uint64_t)c.z * y;
-      t[3] += (uint64_t)c.w * y;
-    }
-    if (!M.multi) {
-#pragma unroll
-      for (int q = 0; q < NS; q++)
-        if (q == (int)M.slot) {
-#pragma unroll
-          for (int l = 0; l < 4; l++) acc[q][l] = L::fold(L::fold(acc[q][l]) + L::fold(t[l]));
-        }
-      continue;
-    }
-    // r = sum_j alpha^j M[i][j]; each (slot, alpha^off) term adds alpha^off * r
-    Ext4 r;
-#pragma unroll
-    for (int l = 0; l < 4; l++) r.c[l] = L::finish(t[l]);
-    for (uint32_t k = 0; k < M.n_terms; k++) {
-      const ReduceTerm T = h.terms[M.term0 + k];
-      const Ext4 a = ld4(h.apow + T.off);
-      constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
-      const uint32_t wa1 = Fp<F>::mul(a.c[1], Wm), wa2 = Fp<F>::mul(a.c[2], Wm), wa3 = Fp<F>::mul(a.c[3], Wm);
-#pragma unroll
-      for (int q = 0; q < NS; q++)
-        if (q == (int)T.slot) {
-          uint64_t* s = acc[q];
-          s[0] = L::fold(s[0]);
-          s[1] = L::fold(s[1]);
-          s[2] = L::fold(s[2]);
-          s[3] = L::fold(s[3]);
-          s[0] += (uint64_t)a.c[0] * r.c[0] + (uint64_t)wa1 * r.c[3] + (uint64_t)wa2 * r.c[2] + (uint64_t)wa3 * r.c[1];
-          s[1] += (uint64_t)a.c[0] * r.c[1] + (uint64_t)a.c[1] * r.c[0] + (uint64_t)wa2 * r.c[3] + (uint64_t)wa3 * r.c[2];
-          s[2] += (uint64_t)a.c[0] * r.c[2] + (uint64_t)a.c[1] * r.c[1] + (uint64_t)a.c[2] * r.c[0] + (uint64_t)wa3 * r.c[3];
-          s[3] += (uint64_t)a.c[0] * r.c[3] + (uint64_t)a.c[1] * r.c[2] + (uint64_t)a.c[2] * r.c[1] + (uint64_t)a.c[3] * r.c[0];
-        }
-    }
+    m = m2;
+    j0 = j2;
+    buf ^= 1;
   }
-  Ext4 res{{0, 0, 0, 0}};
-  if (h.accumulate) res = ld4(h.ro + i);
+  if (lane >= rows) return;
+  // ro[i] (+)= sum_q d_q[i] * (K_q - S_q)
+  uint64_t o[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int q = 0; q < NS; q++) {
-    Ext4 s;
+    Ext4 u;
 #pragma unroll
-    for (int l = 0; l < 4; l++) s.c[l] = L::finish(acc[q][l]);
-    res = E::add(res, E::mul(ld4(h.dinv[q] + i), E::sub(h.K[q], s)));
+    for (int l = 0; l < 4; l++) u.c[l] = B::sub(h.K[q].c[l], L::finish(acc[q][l]));
+    const Ext4 d = ld4(h.dinv[q] + i);
+    const uint32_t wd[4] = {0, B::mul(d.c[1], Wm), B::mul(d.c[2], Wm), B::mul(d.c[3], Wm)};
+    lazy_ef_mac<F>(o, d.c, wd, u);
   }
+  Ext4 res;
+#pragma unroll
+  for (int l = 0; l < 4; l++) res.c[l] = L::finish(o[l]);
+  if (h.accumulate) res = E::add(res, ld4(h.ro + i));
   h.ro[i] = st4(res);
 }
 
 template <class F>
 static cudaError_t launch_reduce_t(const ReduceHeight& h, cudaStream_t st) {
   const uint64_t n = 1ull << h.log_h;
-  const unsigned blocks = (unsigned)((n + 255) / 256);
+  const unsigned rows_per_block = 32 * kReduceWarps;
+  const unsigned blocks = (unsigned)((n + rows_per_block - 1) / rows_per_block);
+  const unsigned threads = 32 * kReduceWarps;
   switch (h.n_slots) {
-    case 1: k_reduce<F, 1><<<blocks, 256, 0, st>>>(h); break;
-    case 2: k_reduce<F, 2><<<blocks, 256, 0, st>>>(h); break;
-    case 3: k_reduce<F, 3><<<blocks, 256, 0, st>>>(h); break;
-    case 4: k_reduce<F, 4><<<blocks, 256, 0, st>>>(h); break;
+    case 1: k_reduce<F, 1><<<blocks, threads, 0, st>>>(h); break;
+    case 2: k_reduce<F, 2><<<blocks, threads, 0, st>>>(h); break;
+    case 3: k_reduce<F, 3><<<blocks, threads, 0, st>>>(h); break;
+    case 4: k_reduce<F, 4><<<blocks, threads, 0, st>>>(h); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
