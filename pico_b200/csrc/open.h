@@ -35,7 +35,7 @@ struct ReduceMat {
   uint32_t multi;    // 0: one point (slot, off); 1: n_terms terms from term0
   uint32_t slot, off;
   uint32_t n_terms, term0;
-  uint32_t vec;      // rows 16-byte aligned and w % 4 == 0: 16-byte loads
+  uint32_t vec;      // the matrix starts 16-byte aligned (16-byte copies where rows allow)
   uint32_t pad;
 };
 // One (point, alpha^off) term of a matrix opened at several points: a = alpha^off

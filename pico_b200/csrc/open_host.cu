@@ -399,7 +399,7 @@ struct Opening {
               R.lde = c->lde[a.m];
               R.w = c->width[a.m];
               R.magic = ((1ull << 32) + R.w - 1) / R.w;
-              R.vec = (R.w % 4 == 0 && ((uintptr_t)R.lde & 15) == 0) ? 1u : 0u;
+              R.vec = ((uintptr_t)R.lde & 15) == 0 ? 1u : 0u;
               if (terms.size() == 1) {
                 R.multi = 0;
                 R.slot = terms[0].slot;

@@ -387,63 +387,90 @@ __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_
 // Copy tile j0 of matrix M (rows row0 .. row0 + rows - 1, columns j0 .. j0 + 31)
 // into `tile` with asynchronous copies; a matrix of at most 32 columns is one
 // tile taken as its rows * w contiguous words.
+// Tile forms.  A matrix of at most 32 columns is one tile holding its 32 rows:
+// with w % 4 == 0 in padded rows (stride kTileStride, 16-byte copies and reads);
+// otherwise as the rows * w contiguous words they are in memory (16-byte
+// copies when the matrix is 16-byte aligned; lane l reads row l at stride w:
+// odd w is conflict-free, w = 2 mod 4 two-way).  Wider matrices: tiles of 32
+// columns in padded rows.
+__device__ __forceinline__ bool tile_flat(const ReduceMat& M) { return M.w <= 32 && !(M.w % 4 == 0 && M.vec); }
+
 __device__ __forceinline__ void issue_tile(const ReduceMat& M, const uint4* apow, uint32_t apow_len, uint64_t N,
                                            uint64_t row0, uint32_t rows, uint32_t j0, uint32_t* tile, uint32_t lane) {
   const uint32_t w = M.w;
-  {
-    // the tile's alpha powers: alpha^(off + j0 + lane) (one point) or alpha^(j0 + lane)
-    const uint32_t cw = w <= 32 ? w : min(32u, w - j0);
-    const uint32_t k = (M.multi ? 0u : M.off) + j0 + lane;
-    if (lane < cw) {
-      if (k < apow_len)
-        cp_async16(tile + kTileWords + 4 * lane, reinterpret_cast<const uint32_t*>(apow + k));
-      else
-        open_guard_trip(kGuardTwiddle, k, apow_len);
-    }
-  }
+  const uint32_t cw = w <= 32 ? w : min(32u, w - j0);
   const uint32_t* src = M.lde + row0 * w;
   const uint64_t limit = N * w;  // words of the matrix
-  // checked copy: word `so` of the matrix (from src) to word `dofs` of the tile
-  auto copy = [&](uint32_t dofs, uint64_t so, uint32_t words) {
-    const uint64_t g = row0 * w + so;
-    if (dofs + words > (uint32_t)kTileWords || g + words > limit) {
-      open_guard_trip(kGuardTile, dofs, g);
+  // every copy checked: tile slot (data or power part), matrix word, 16-byte alignment
+  auto copy = [&](uint32_t dofs, const uint32_t* from, uint64_t from_word, uint64_t from_limit, uint32_t words) {
+    if (dofs + words > (uint32_t)kTileBufWords || from_word + words > from_limit) {
+      open_guard_trip(kGuardTile, dofs, from_word);
       return;
     }
     if (words == 4) {
-      if ((((uintptr_t)(tile + dofs)) | ((uintptr_t)(src + so))) & 15u) {
-        open_guard_trip(kGuardLoad, dofs, g);
+      if ((((uintptr_t)(tile + dofs)) | ((uintptr_t)from)) & 15u) {
+        open_guard_trip(kGuardLoad, dofs, from_word);
         return;
       }
-      cp_async16(tile + dofs, src + so);
+      cp_async16(tile + dofs, from);
     } else {
-      cp_async4(tile + dofs, src + so);
+      cp_async4(tile + dofs, from);
     }
   };
+  // the tile's alpha powers: alpha^(off + j0 + lane) (one point) or alpha^(j0 + lane)
+  const uint32_t k0 = (M.multi ? 0u : M.off) + j0;
+  if (lane < cw)
+    copy(kTileWords + 4 * lane, reinterpret_cast<const uint32_t*>(apow + k0 + lane), 4ull * (k0 + lane),
+         4ull * apow_len, 4);
   if (w <= 32) {
     const uint32_t total = rows * w;
-    if (M.vec) {
+    if (!tile_flat(M)) {
+      // w % 4 == 0, aligned: padded rows, one 16-byte copy per lane step
       for (uint32_t f = 4 * lane; f < total; f += 4 * 32) {
         const uint32_t r = (uint32_t)(((uint64_t)f * M.magic) >> 32);  // f / w
-        copy(r * kTileStride + (f - r * w), f, 4);
+        copy(r * kTileStride + (f - r * w), src + f, row0 * w + f, limit, 4);
       }
+    } else if (M.vec) {
+      const uint32_t quads = total >> 2;
+      for (uint32_t q = lane; q < quads; q += 32) copy(4 * q, src + 4 * q, row0 * w + 4 * q, limit, 4);
+      for (uint32_t f = 4 * quads + lane; f < total; f += 32) copy(f, src + f, row0 * w + f, limit, 1);
     } else {
-      for (uint32_t f = lane; f < total; f += 32) {
-        const uint32_t r = (uint32_t)(((uint64_t)f * M.magic) >> 32);
-        copy(r * kTileStride + (f - r * w), f, 1);
-      }
+      for (uint32_t f = lane; f < total; f += 32) copy(f, src + f, row0 * w + f, limit, 1);
     }
     return;
   }
-  const uint32_t cw = min(32u, w - j0);
-  if (M.vec) {
+  if (M.vec && w % 4 == 0) {
     // eight lanes per row, four rows per step; cw is a multiple of 4
     const uint32_t rr = lane >> 3, q = (lane & 7) * 4;
     if (q < cw)
-      for (uint32_t r = rr; r < rows; r += 4) copy(r * kTileStride + q, (uint64_t)r * w + j0 + q, 4);
+      for (uint32_t r = rr; r < rows; r += 4) {
+        const uint64_t o = (uint64_t)r * w + j0 + q;
+        copy(r * kTileStride + q, src + o, row0 * w + o, limit, 4);
+      }
   } else if (lane < cw) {
-    for (uint32_t r = 0; r < rows; r++) copy(r * kTileStride + lane, (uint64_t)r * w + j0 + lane, 1);
+    for (uint32_t r = 0; r < rows; r++) {
+      const uint64_t o = (uint64_t)r * w + j0 + lane;
+      copy(r * kTileStride + lane, src + o, row0 * w + o, limit, 1);
+    }
   }
+}
+
+// t += sum_j coef[j] * row[j], the row at stride 1 but without 16-byte alignment
+template <class F>
+__device__ __forceinline__ void lazy_row_flat(uint64_t t[4], const uint32_t* tile_row, const uint4* coef, uint32_t cw) {
+  uint32_t j = 0;
+  for (; j + 4 <= cw; j += 4) {
+    const uint32_t y0 = tile_row[j], y1 = tile_row[j + 1], y2 = tile_row[j + 2], y3 = tile_row[j + 3];
+    mac4<F>(t, coef[j], y0);
+    mac4<F>(t, coef[j + 1], y1);
+    mac4<F>(t, coef[j + 2], y2);
+    mac4<F>(t, coef[j + 3], y3);
+#pragma unroll
+    for (int l = 0; l < 4; l++) t[l] = Lazy<F>::fold(t[l]);
+  }
+  for (; j < cw; j++) mac4<F>(t, coef[j], tile_row[j]);
+#pragma unroll
+  for (int l = 0; l < 4; l++) t[l] = Lazy<F>::fold(t[l]);
 }
 
 // Lane l of a warp owns row row0 + l.  The warp walks the tiles of all
@@ -487,7 +514,10 @@ __global__ void __launch_bounds__(32 * kReduceWarps, 5) k_reduce(ReduceHeight h)
     __syncwarp();
     const uint32_t cw = M.w <= 32 ? M.w : min(32u, M.w - j0);
     const uint4* coef = reinterpret_cast<const uint4*>(tiles[warp][buf] + kTileWords);
-    lazy_row_tile<F>(t, tiles[warp][buf] + lane * kTileStride, coef, cw);
+    if (tile_flat(M))
+      lazy_row_flat<F>(t, tiles[warp][buf] + lane * M.w, coef, cw);
+    else
+      lazy_row_tile<F>(t, tiles[warp][buf] + lane * kTileStride, coef, cw);
     __syncwarp();  // the buffer is refilled next iteration
     if (m2 != m) {
       // matrix m done
