@@ -71,8 +71,15 @@ typedef struct {
   uint32_t log_height;
   uint32_t width;
   uint32_t shift; /* LDE coset shift, Monty form: GENERATOR / domain.shift */
-  uint32_t reserved;
+  uint32_t flags; /* PICO_MATRIX_* */
 } pico_matrix;
+
+/* pico_matrix.flags: the values are degree-4 extension elements (4 Monty words
+ * each, c0..c3) and `width` counts them.  The matrix is committed as the base
+ * matrix of 4 * width columns that flatten_to_base makes of it (the
+ * permutation traces, vm/src/machine/prover.rs:404-415) -- the same words, so
+ * nothing is copied or rearranged. */
+#define PICO_MATRIX_EXT4 0x1u
 
 typedef struct {
   uint64_t hbm_budget_bytes; /* admission budget; 0 = 90% of free HBM at init */
@@ -137,6 +144,13 @@ pico_status pico_gpu_last_commit_stats(pico_commit_stats *out);
  * PICO_OUTPUT_DEVICE. */
 pico_status pico_gpu_lde_rows(pico_ctx *ctx, const pico_commit *c, uint32_t mat_idx, uint64_t row_begin,
                               uint64_t row_end, uint32_t *out, uint32_t flags);
+/* Pcs::get_evaluations_on_domain for the domain g * H_(2^log_domain), no taller
+ * than the committed LDE (the quotient-domain reads of compute_quotient_values,
+ * vm/src/machine/prover.rs:469-489): the first 2^log_domain committed rows,
+ * returned in natural order (row k = evaluation at g * w^k), row-major
+ * 2^log_domain x width words; host memory unless PICO_OUTPUT_DEVICE. */
+pico_status pico_gpu_evaluations_on_domain(pico_ctx *ctx, const pico_commit *c, uint32_t mat_idx,
+                                           uint32_t log_domain, uint32_t *out, uint32_t flags);
 /* Shape of a committed LDE: log2 height and width. */
 pico_status pico_gpu_lde_shape(const pico_commit *c, uint32_t mat_idx, uint32_t *log_height, uint32_t *width);
 /* Digest layer `level` (0 = leaves) of the commit's tree: 2^(log_max - level)

@@ -42,13 +42,16 @@ class PicoError(RuntimeError):
         self.status = status
 
 
+PICO_MATRIX_EXT4 = 0x1
+
+
 class Matrix(C.Structure):
     _fields_ = [
         ("values", C.c_void_p),
         ("log_height", C.c_uint32),
         ("width", C.c_uint32),
         ("shift", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("flags", C.c_uint32),
     ]
 
 
@@ -140,6 +143,7 @@ SIGNATURES = {
     "pico_gpu_last_commit_stats": (C.c_int, [C.POINTER(CommitStats)]),
     "pico_gpu_lde_rows": (C.c_int, [_vp, _vp, _u32, _u64, _u64, _vp, _u32]),
     "pico_gpu_lde_shape": (C.c_int, [_vp, _u32, _u32p, _u32p]),
+    "pico_gpu_evaluations_on_domain": (C.c_int, [_vp, _vp, _u32, _u32, _vp, _u32]),
     "pico_gpu_digest_layer": (C.c_int, [_vp, _vp, _u32, _vp, _u32]),
     "pico_gpu_open_batch": (C.c_int, [_vp, _vp, _u64, _vp, _vp]),
     "pico_gpu_coset_lde_batch": (C.c_int, [_vp, C.c_int, _vp, _u32, _u32, _u32, _u32, _vp, _u32]),

@@ -395,15 +395,25 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
       set_error("commit: matrix %u has null values", i);
       return PICO_ERR_INVALID_ARG;
     }
+    if (m.flags & ~PICO_MATRIX_EXT4) {
+      set_error("commit: matrix %u has unknown flags 0x%x", i, m.flags);
+      return PICO_ERR_INVALID_ARG;
+    }
+    // an extension-field matrix is committed as its base flattening: 4 words per element
+    const uint64_t base_w = (uint64_t)m.width * ((m.flags & PICO_MATRIX_EXT4) ? 4u : 1u);
+    if (base_w > 0xffffffffull) {
+      set_error("commit: matrix %u is too wide", i);
+      return PICO_ERR_INVALID_ARG;
+    }
     PlannedMat pm;
     pm.input_idx = i;
     pm.log_n = m.log_height;
     pm.log_N = m.log_height + plan.log_b;
-    pm.w = m.width;
+    pm.w = (uint32_t)base_w;
     pm.shift = m.shift;
     pm.src = m.values;
     plan.mats.push_back(pm);
-    plan.cells += (uint64_t)m.width << m.log_height;
+    plan.cells += base_w << m.log_height;
   }
   std::stable_sort(plan.mats.begin(), plan.mats.end(),
                    [](const PlannedMat& a, const PlannedMat& b) { return a.log_N > b.log_N; });

@@ -81,6 +81,8 @@ cudaError_t launch_reduce(int field, const ReduceHeight& h, cudaStream_t st);
 // Bounds guard of the reduction's tile copies (synchronous read-back / clear).
 cudaError_t open_guard_fetch(GuardRecord* dst);
 cudaError_t open_guard_clear();
+// out row k = lde row rev(k), k < 2^log_d (rows of w words)
+cudaError_t launch_domain_rows(const uint32_t* lde, uint32_t w, uint32_t log_d, uint32_t* out, cudaStream_t st);
 cudaError_t launch_gather_queries(const QuerySeg* segs, uint32_t n_segs, const uint32_t* indices, uint32_t n_queries,
                                   uint64_t query_words, uint32_t* out, cudaStream_t st);
 

@@ -806,3 +806,46 @@ extern "C" pico_status pico_gpu_reduced_opening(pico_ctx* ctx, const pico_open_b
     return reduced_opening_t<KoalaBear>(ctx, batches, n_batches, log_blowup, sh, values, alpha, log_height, out);
   return reduced_opening_t<BabyBear>(ctx, batches, n_batches, log_blowup, sh, values, alpha, log_height, out);
 }
+
+extern "C" pico_status pico_gpu_evaluations_on_domain(pico_ctx* ctx, const pico_commit* c, uint32_t mat_idx,
+                                                      uint32_t log_domain, uint32_t* out, uint32_t flags) {
+  if (!ctx || !c || c->ctx != ctx || !out || mat_idx >= c->n_mats) {
+    set_error("evaluations_on_domain: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (log_domain > c->log_N[mat_idx]) {
+    set_error("evaluations_on_domain: domain 2^%u is taller than the committed LDE 2^%u", log_domain,
+              c->log_N[mat_idx]);
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint32_t w = c->width[mat_idx];
+  const uint64_t bytes = ((uint64_t)w << log_domain) * 4;
+  if (bytes == 0) return PICO_OK;
+  cudaSetDevice(ctx->device);
+  uint32_t slot = 0;
+  cudaStream_t st = pick_stream(ctx, nullptr, &slot);
+  const bool dev_out = (flags & PICO_OUTPUT_DEVICE) != 0;
+  if (!dev_out && !try_reserve(ctx, bytes)) {
+    set_error("evaluations_on_domain: HBM budget exceeded");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  void* tmp = nullptr;
+  auto run = [&]() -> pico_status {
+    pico_status s;
+    uint32_t* dst = out;
+    if (!dev_out) {
+      if ((s = cuda_status(cudaMallocAsync(&tmp, bytes, st), "device allocation"))) return s;
+      dst = (uint32_t*)tmp;
+    }
+    if ((s = cuda_status(launch_domain_rows(c->lde[mat_idx], w, log_domain, dst, st), "domain rows"))) return s;
+    if (!dev_out)
+      return cuda_status(cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, st), "read-back");
+    return PICO_OK;
+  };
+  pico_status s = run();
+  if (tmp) cudaFreeAsync(tmp, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (!s) s = cuda_status(e, "evaluations_on_domain");
+  if (!dev_out) unreserve(ctx, bytes);
+  return s;
+}

@@ -589,6 +589,24 @@ cudaError_t launch_reduce(int field, const ReduceHeight& h, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
+// Evaluations on a domain: out row k = committed row rev(k) (k < 2^log_d), one
+// warp per row, lanes across the columns.
+__global__ void k_domain_rows(const uint32_t* lde, uint32_t w, uint32_t log_d, uint32_t* out) {
+  const uint64_t k = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (k >= (1ull << log_d)) return;
+  const uint32_t* src = lde + bitrev64(k, (int)log_d) * w;
+  uint32_t* dst = out + k * w;
+  for (uint32_t j = lane; j < w; j += 32) dst[j] = __ldg(src + j);
+}
+
+cudaError_t launch_domain_rows(const uint32_t* lde, uint32_t w, uint32_t log_d, uint32_t* out, cudaStream_t st) {
+  const uint64_t threads = 32ull << log_d;
+  k_domain_rows<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(lde, w, log_d, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Query records: one block per query, one warp per segment.
 __global__ void k_gather_queries(const QuerySeg* segs, uint32_t n_segs, const uint32_t* indices, uint64_t query_words,
                                  uint32_t* out) {

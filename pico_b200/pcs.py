@@ -145,6 +145,16 @@ class ProverData:
         abi.check(self.ctx.lib.pico_gpu_lde_rows(self.ctx.handle, self.handle, i, begin, end, _ptr(out), flags))
         return out
 
+    def evaluations_on_domain(self, i: int, log_domain: int, out=None):
+        """Pcs::get_evaluations_on_domain for g * H_(2^log_domain): natural row order."""
+        _, w = self.lde_shape(i)
+        if out is None:
+            out = np.zeros((1 << log_domain, w), dtype=np.uint32)
+        flags = abi.PICO_OUTPUT_DEVICE if _is_device(out) else 0
+        abi.check(self.ctx.lib.pico_gpu_evaluations_on_domain(self.ctx.handle, self.handle, i, log_domain,
+                                                               _ptr(out), flags))
+        return out
+
     def lde(self, i: int):
         return self.lde_rows(i)
 
@@ -325,10 +335,15 @@ class TwoAdicFriPcs:
         for k, (dom, t) in enumerate(domains_and_traces):
             if t.shape[0] != 1 << dom.log_n:
                 raise ValueError(f"trace {k}: height {t.shape[0]} != domain size {1 << dom.log_n}")
+            ext = len(t.shape) == 3
+            if ext and t.shape[2] != 4:
+                raise ValueError(f"trace {k}: extension traces have 4 words per element")
             mats[k].values = _ptr(t)
             mats[k].log_height = dom.log_n
             mats[k].width = t.shape[1]
             mats[k].shift = F.lde_shift(self.field, dom.shift)
+            # (n, w, 4) extension traces commit as their base flattening (flatten_to_base)
+            mats[k].flags = abi.PICO_MATRIX_EXT4 if ext else 0
         root = np.zeros(8, dtype=np.uint32)
         h = C.c_void_p()
         abi.check(self.ctx.lib.pico_gpu_commit(

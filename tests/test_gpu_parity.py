@@ -335,3 +335,39 @@ def test_serving_results_match_alone(gpu, orc):
         pd.release()
         r.free()
     assert gpu.memory()[0] == 0
+
+
+# ------------------------------------------- extension traces, domain reads
+@pytest.mark.parametrize("f", FIELDS)
+def test_extension_trace_commits_as_its_flattening(gpu, orc, f):
+    """A permutation trace of EF4 elements (prover.rs:404-415) commits as
+    flatten_to_base makes it: each element's c0..c3 in place, 4w base columns."""
+    pcs = TwoAdicFriPcs(gpu, f, 1)
+    ext = [F.random_matrix(f, lh, 4 * w, 700 + lh).reshape(1 << lh, w, 4) for lh, w in ((6, 3), (4, 5), (6, 1))]
+    flat = [np.ascontiguousarray(e.reshape(e.shape[0], -1)) for e in ext]
+    doms = [pcs.natural_domain_for_degree(e.shape[0]) for e in ext]
+    root_ext, pd = pcs.commit(list(zip(doms, ext)))
+    root_flat, _ = pcs.commit(list(zip(doms, flat)), keep=False)
+    want, _, _ = orc.pcs_commit(f, flat, [F.lde_shift(f)] * len(flat), 1)
+    assert (root_ext == want).all() and (root_flat == want).all()
+    assert pd.lde_shape(0) == (128, 12)
+
+
+@pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("log_n,b,extra", [(5, 1, 1), (5, 1, 0), (6, 2, 1), (6, 2, 2), (4, 2, -1), (0, 1, 1)])
+def test_evaluations_on_domain(gpu, orc, f, log_n, b, extra):
+    """get_evaluations_on_domain(g * H_(2^(log_n + extra))): natural-order
+    evaluations, i.e. the natural-order coset LDE at stride 2^(b - extra)."""
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    t = F.random_matrix(f, log_n, 3, 900 + log_n)
+    _, pd = pcs.commit([(pcs.natural_domain_for_degree(1 << log_n), t)])
+    ld = log_n + extra
+    got = pd.evaluations_on_domain(0, ld)
+    nat = orc.coset_lde(f, t, b, F.lde_shift(f), bitrev=False)
+    assert np.array_equal(got, nat[:: 1 << (log_n + b - ld)])
+    torch = _torch()
+    dev = torch.zeros((1 << ld, 3), dtype=torch.int32, device="cuda")
+    pd.evaluations_on_domain(0, ld, out=dev)
+    assert np.array_equal(dev.cpu().numpy().view(np.uint32), got)
+    with pytest.raises(PicoError):
+        pd.evaluations_on_domain(0, log_n + b + 1)
