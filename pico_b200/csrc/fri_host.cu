@@ -19,34 +19,49 @@ using namespace pico;
 namespace pico {
 pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& tw, uint32_t log_n, uint32_t R,
                                const std::vector<uint32_t*>& codewords, const std::vector<uint32_t*>& trees,
-                               uint32_t* d_betas, DevChallenger* d_ch, const uint32_t* const* inject) {
+                               uint32_t* d_betas, DevChallenger* d_ch, const uint32_t* const* inject,
+                               uint32_t* launches) {
   pico_status s;
+  uint32_t nl = 0;
   for (uint32_t r = 0; r < R; r++) {
     const uint32_t L = log_n - r;            // codeword length 2^L
     const uint64_t leaves = 1ull << (L - 1);  // rows of the (len/2) x 8 matrix
-    RowGroup g;
-    memset(&g, 0, sizeof g);
-    g.n_segs = 1;
-    g.total_width = 8;
-    g.segs[0].ptr = codewords[r];
-    g.segs[0].width = 8;
-    uint32_t* layer = trees[r];
-    if ((s = cuda_status(launch_hash_rows(field, g, leaves, layer, st), "FRI leaf hashing"))) return s;
-    for (uint32_t lvl = 1; lvl < L; lvl++) {
-      const uint64_t len = leaves >> lvl;
-      uint32_t* next = layer + 2 * len * 8;
-      if ((s = cuda_status(launch_compress(field, layer, next, len, nullptr, st), "FRI compression"))) return s;
-      layer = next;
+    if (r == 0) {
+      // later rounds' leaves come out of the previous round's fold
+      RowGroup g;
+      memset(&g, 0, sizeof g);
+      g.n_segs = 1;
+      g.total_width = 8;
+      g.segs[0].ptr = codewords[0];
+      g.segs[0].width = 8;
+      if ((s = cuda_status(launch_hash_rows(field, g, leaves, trees[0], st), "FRI leaf hashing"))) return s;
+      nl++;
     }
-    // layer now points at the root
-    if (d_ch)
-      if ((s = cuda_status(launch_challenger_round(field, d_ch, layer, d_betas + 4 * r, st), "challenger")))
-        return s;
-    if ((s = cuda_status(launch_fri_fold_tw(field, codewords[r], L, d_betas + 4 * r, tw, codewords[r + 1], st,
-                                            inject ? inject[r] : nullptr),
-                         "fold")))
+    // wide levels one launch each, the last 512 nodes and the challenger in one block
+    uint32_t* layer = trees[r];
+    uint64_t n = leaves;
+    while (n > 512) {
+      uint32_t* next = layer + n * 8;
+      if ((s = cuda_status(launch_compress(field, layer, next, n / 2, nullptr, st), "FRI compression"))) return s;
+      nl++;
+      layer = next;
+      n /= 2;
+    }
+    if ((s = cuda_status(launch_tree_top(field, layer, (uint32_t)n, d_ch, d_betas + 4 * r, st), "FRI tree top")))
       return s;
+    nl++;
+    const uint32_t* inj = inject ? inject[r] : nullptr;
+    if (r + 1 < R)
+      s = cuda_status(launch_fri_fold_hash(field, codewords[r], L, d_betas + 4 * r, tw, codewords[r + 1], inj,
+                                           trees[r + 1], st),
+                      "fold and hash");
+    else
+      s = cuda_status(launch_fri_fold_tw(field, codewords[r], L, d_betas + 4 * r, tw, codewords[r + 1], st, inj),
+                      "fold");
+    if (s) return s;
+    nl++;
   }
+  if (launches) *launches = nl;
   return PICO_OK;
 }
 }  // namespace pico
@@ -141,7 +156,7 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
         return s;
     }
     if ((s = enqueue_fri_rounds(field, st, tw, log_n, R, f->codewords, f->trees, d_betas, betas_in ? nullptr : d_ch,
-                                nullptr)))
+                                nullptr, nullptr)))
       return s;
     // Read-backs are queued after the whole loop: a copy into pageable host
     // memory blocks the calling thread until the stream reaches it.

@@ -88,6 +88,11 @@ cudaError_t launch_stage_tables(int field, TwiddleTables tw, uint32_t* stage, cu
 // TwoAdicFriPcs::open, mirrored by fri.rs:300-318).
 cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
                                TwiddleTables tw, uint32_t* out, cudaStream_t st, const uint32_t* inject = nullptr);
+// Fold (as launch_fri_fold_tw, with inject) and hash the folded codeword's
+// leaves: leaves[k] = hash(out[2k] || out[2k+1]) (8 words), log_len >= 2.
+cudaError_t launch_fri_fold_hash(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
+                                 TwiddleTables tw, uint32_t* out, const uint32_t* inject, uint32_t* leaves,
+                                 cudaStream_t st);
 // Coefficients of the final polynomial (2^log_keep x 4 words) from the last
 // codeword of 2^log_len EF4 elements; *err set if higher coefficients are nonzero.
 cudaError_t launch_fri_final_poly(int field, const uint32_t* cw, uint32_t log_len, uint32_t log_keep,
@@ -95,6 +100,10 @@ cudaError_t launch_fri_final_poly(int field, const uint32_t* cw, uint32_t log_le
 // Observe an 8-element root, then sample 4 elements into beta_out (EF4).
 cudaError_t launch_challenger_round(int field, DevChallenger* ch, const uint32_t* root, uint32_t* beta_out,
                                     cudaStream_t st);
+// Levels above `level` (n_in <= 512 digests, a power of two) up to the root,
+// written after it; with ch, then observe the root and sample beta_out (4 words).
+cudaError_t launch_tree_top(int field, uint32_t* level, uint32_t n_in, DevChallenger* ch, uint32_t* beta_out,
+                            cudaStream_t st);
 // Observe n elements at vals.
 cudaError_t launch_challenger_observe(int field, DevChallenger* ch, const uint32_t* vals, uint32_t n,
                                       cudaStream_t st);

@@ -538,10 +538,11 @@ pico_status pcs_open_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_t n
     static_assert(sizeof(DevChallenger) == sizeof(pico_challenger), "challenger layout");
     if ((s = cuda_status(cudaMemcpyAsync(d_ch, &tr, sizeof tr, cudaMemcpyHostToDevice, O.st), "challenger")))
       return s;
+    uint32_t fri_launches = 0;
     if ((s = enqueue_fri_rounds(F::ID, O.st, twiddles(ctx, F::ID), log_max, R, cws, trees, d_betas, d_ch,
-                                inject.data())))
+                                inject.data(), &fri_launches)))
       return s;
-    for (uint32_t r = 0; r < R; r++) O.launches += (log_max - r) + 2;  // hash, compressions, challenger, fold
+    O.launches += fri_launches;
     if ((s = cuda_status(launch_challenger_observe(F::ID, d_ch, cws[R], 4, O.st), "observe final"))) return s;
     O.launches++;
     if ((s = tm.mark(O.st))) return s;

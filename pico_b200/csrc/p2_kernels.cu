@@ -270,16 +270,10 @@ cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uin
 //   (lo + hi)/2 + (beta/2) * g_inv^rev(r) * (lo - hi),
 // g = two_adic_generator(log len), rev over log(len/2) bits.
 template <class F>
-__global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t* beta, TwiddleTables tw,
-                           uint32_t* out, const uint32_t* inject) {
+__device__ __forceinline__ Ext4 fri_fold_row(const uint32_t* cw, uint32_t log_len, uint64_t r, const Ext4& hb,
+                                             const TwiddleTables& tw) {
   using B = Fp<F>;
   using E = Ef<F>;
-  const uint64_t h = 1ull << (log_len - 1);
-  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (r >= h) return;
-  Ext4 hb;
-#pragma unroll
-  for (int i = 0; i < 4; i++) hb.c[i] = B::half(__ldg(beta + i));
   // g_inv^rev(r) = w_max^(-(rev(r) << (S - log_len)))
   const uint32_t mask = (1u << F::TWO_ADICITY) - 1u;
   uint32_t e = (uint32_t)bitrev64(r, (int)log_len - 1) << (F::TWO_ADICITY - log_len);
@@ -293,11 +287,73 @@ __global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t*
   Ext4 pd = E::mul(hb, E::scale(dif, t));
 #pragma unroll
   for (int i = 0; i < 4; i++) res.c[i] = B::add(B::half(sum.c[i]), pd.c[i]);
+  return res;
+}
+
+template <class F>
+__device__ __forceinline__ Ext4 half_beta(const uint32_t* beta) {
+  Ext4 hb;
+#pragma unroll
+  for (int i = 0; i < 4; i++) hb.c[i] = Fp<F>::half(__ldg(beta + i));
+  return hb;
+}
+
+template <class F>
+__global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t* beta, TwiddleTables tw,
+                           uint32_t* out, const uint32_t* inject) {
+  const uint64_t h = 1ull << (log_len - 1);
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= h) return;
+  Ext4 res = fri_fold_row<F>(cw, log_len, r, half_beta<F>(beta), tw);
   if (inject) {
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(inject) + r);
-    res = E::add(res, Ext4{{v.x, v.y, v.z, v.w}});
+    res = Ef<F>::add(res, Ext4{{v.x, v.y, v.z, v.w}});
   }
   reinterpret_cast<uint4*>(out)[r] = make_uint4(res.c[0], res.c[1], res.c[2], res.c[3]);
+}
+
+// Fold, then hash the next round's leaves in the same pass: thread k folds
+// rows 2k and 2k+1 (adding the injected reduced opening), stores them, and
+// hashes the pair as one 8-element leaf (one permutation: the rate block is
+// the row, PaddingFreeSponge over 8 elements).
+template <class F>
+__global__ void __launch_bounds__(256) k_fri_fold_hash(const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
+                                                       TwiddleTables tw, uint32_t* out, const uint32_t* inject,
+                                                       uint32_t* leaves) {
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= (1ull << (log_len - 2))) return;
+  const Ext4 hb = half_beta<F>(beta);
+  uint32_t s[16];
+#pragma unroll
+  for (int u = 0; u < 2; u++) {
+    const uint64_t r = 2 * k + u;
+    Ext4 res = fri_fold_row<F>(cw, log_len, r, hb, tw);
+    if (inject) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(inject) + r);
+      res = Ef<F>::add(res, Ext4{{v.x, v.y, v.z, v.w}});
+    }
+    reinterpret_cast<uint4*>(out)[r] = make_uint4(res.c[0], res.c[1], res.c[2], res.c[3]);
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[4 * u + i] = res.c[i];
+  }
+#pragma unroll
+  for (int i = 8; i < 16; i++) s[i] = 0;
+  p2_permute<F>(s);
+  uint4* lp = reinterpret_cast<uint4*>(leaves + 8 * k);
+  lp[0] = make_uint4(s[0], s[1], s[2], s[3]);
+  lp[1] = make_uint4(s[4], s[5], s[6], s[7]);
+}
+
+cudaError_t launch_fri_fold_hash(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
+                                 TwiddleTables tw, uint32_t* out, const uint32_t* inject, uint32_t* leaves,
+                                 cudaStream_t st) {
+  if (log_len < 2) return cudaErrorInvalidValue;
+  const uint64_t n = 1ull << (log_len - 2);
+  if (field == 0)
+    k_fri_fold_hash<KoalaBear><<<blocks_for(n, 256), 256, 0, st>>>(cw, log_len, beta, tw, out, inject, leaves);
+  else
+    k_fri_fold_hash<BabyBear><<<blocks_for(n, 256), 256, 0, st>>>(cw, log_len, beta, tw, out, inject, leaves);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
@@ -347,6 +403,59 @@ template <class F>
 __global__ void k_challenger_observe(DevChallenger* ch, const uint32_t* vals, uint32_t n) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (uint32_t i = 0; i < n; i++) ch_observe<F>(ch, vals[i]);
+}
+
+// The top of a Merkle tree in one block: `level` holds n_in <= 512 digests
+// (a power of two); every level above it is computed in shared memory and
+// written after it (the layer layout: each level follows the one below), up
+// to the root.  With a challenger, thread 0 then observes the root and samples
+// the EF4 challenge into beta_out (k_challenger_round's step).
+constexpr uint32_t kTreeTopMax = 512;
+
+template <class F>
+__global__ void __launch_bounds__(256) k_tree_top(uint32_t* level, uint32_t n_in, DevChallenger* ch,
+                                                  uint32_t* beta_out) {
+  __shared__ uint32_t buf[kTreeTopMax * 8];
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t i = tid; i < n_in * 8; i += blockDim.x) buf[i] = level[i];
+  __syncthreads();
+  uint32_t n = n_in;
+  uint32_t* in = level;
+  while (n > 1) {
+    const uint32_t m = n >> 1;
+    uint32_t* out = in + (size_t)n * 8;
+    uint32_t s[16];
+    if (tid < m) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) s[k] = buf[16 * tid + k];
+      p2_permute<F>(s);
+    }
+    __syncthreads();
+    if (tid < m) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        buf[8 * tid + k] = s[k];
+        out[8 * tid + k] = s[k];
+      }
+    }
+    __syncthreads();
+    in = out;
+    n = m;
+  }
+  if (ch && tid == 0) {
+    for (int i = 0; i < 8; i++) ch_observe<F>(ch, buf[i]);
+    for (int i = 0; i < 4; i++) beta_out[i] = ch_sample<F>(ch);
+  }
+}
+
+cudaError_t launch_tree_top(int field, uint32_t* level, uint32_t n_in, DevChallenger* ch, uint32_t* beta_out,
+                            cudaStream_t st) {
+  if (n_in == 0 || n_in > kTreeTopMax || (n_in & (n_in - 1))) return cudaErrorInvalidValue;
+  if (field == 0)
+    k_tree_top<KoalaBear><<<1, 256, 0, st>>>(level, n_in, ch, beta_out);
+  else
+    k_tree_top<BabyBear><<<1, 256, 0, st>>>(level, n_in, ch, beta_out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_challenger_round(int field, DevChallenger* ch, const uint32_t* root, uint32_t* beta_out,

@@ -71,14 +71,17 @@ void free_commit_buffers(pico_commit* c, cudaStream_t st);
 // units' records into the slot's pinned host records on st; after st has
 // been synchronised, guard_verdict returns PICO_OK, or an error naming the
 // first skipped access (and clears the device records).
-// FRI commit-phase rounds on st (fri_host.cu): round r hashes codewords[r]
-// as a (len/2) x 8 matrix into trees[r], compresses it to its root, samples
-// beta into d_betas[r] with the device challenger (d_ch null: d_betas holds
-// the challenges already), and folds into codewords[r + 1], adding
-// inject[r] when that is non-null.
+// FRI commit-phase rounds on st (fri_host.cu): round r's tree over
+// codewords[r] viewed as a (len/2) x 8 matrix goes into trees[r] (the leaves of
+// round 0 hashed first, those of later rounds by the previous fold), its root
+// is observed and beta sampled into d_betas[r] by the device challenger (d_ch
+// null: d_betas holds the challenges already), and the fold writes
+// codewords[r + 1], adding inject[r] when that is non-null.  *launches counts
+// the kernels.
 pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& tw, uint32_t log_n, uint32_t R,
                                const std::vector<uint32_t*>& codewords, const std::vector<uint32_t*>& trees,
-                               uint32_t* d_betas, DevChallenger* d_ch, const uint32_t* const* inject);
+                               uint32_t* d_betas, DevChallenger* d_ch, const uint32_t* const* inject,
+                               uint32_t* launches = nullptr);
 pico_status guard_enqueue(pico_ctx* ctx, uint32_t slot, cudaStream_t st);
 pico_status guard_verdict(pico_ctx* ctx, uint32_t slot, std::string* msg = nullptr);
 pico_status finish_stats(pico_commit* c);
