@@ -543,10 +543,11 @@ def run_open(args, rank, world, local):
     st = outs[-1]["stats"]
     proof_bytes = 4 * (outs[-1]["values"].size + outs[-1]["roots"].size + outs[-1]["queries"].size + 4 + 1 + nq)
 
-    # roofline of the reduction: committed cells read once, per row the inverse
-    # denominators of both points read and the reduced opening written
+    # roofline of the reduction phase: the low-coset cells read once, the
+    # inverse denominators of both points read per low-coset row, and the
+    # reduced opening (extended from the low coset) written per committed row
     heights = sorted({lh + b for lh, _ in shapes})
-    red_bytes = 4 * st["reduce_cells"] + sum((1 << h) * 16 * (2 + 1) for h in heights)
+    red_bytes = 4 * st["reduce_cells"] + sum((1 << (h - b)) * 16 * 2 + (1 << h) * 16 for h in heights)
     hbm_peak, hbm_kind = peaks()
     red_ach = red_bytes / (st["ms_reduce"] / 1e3) / 1e9
     val_bytes = 4 * st["value_cells"] // 2 + sum(16 * (1 << lh) * 2 for lh, _ in shapes)
@@ -590,7 +591,8 @@ def run_open(args, rank, world, local):
         "clocks": clocks,
         "phases_ms": {k: st[k] for k in ("ms_values", "ms_reduce", "ms_fri", "ms_grind", "ms_queries", "ms_total")},
         "roofline": {
-            "kernel": "k_reduce (reduced openings, one launch per height)", "bound": "hbm",
+            "kernel": "reduction phase: k_reduce and k_reduce_combine over the low coset, LDE of the result",
+            "bound": "hbm",
             "achieved": red_ach, "peak": hbm_peak, "unit": "GB/s", "frac": red_ach / hbm_peak, "traffic": None,
             "algorithmic_bytes": red_bytes, "launch_ms": st["ms_reduce"],
             "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback"},

@@ -276,7 +276,11 @@ pico_status pico_gpu_open_values(pico_ctx *ctx, const pico_open_batch *batches, 
                                  uint32_t log_blowup, uint32_t *values);
 
 /* The reduced opening of LDE height 2^log_height (2^log_height x 4 words) for
- * the given opened values and alpha, as fed to the commit phase. */
+ * the given opened values and alpha, as fed to the commit phase.  It is formed
+ * on the low coset and extended (it is a polynomial of degree < n there), which
+ * is the reference's row-by-row value when `values` are the opened values
+ * pico_gpu_open_values returns.  A point on a committed coset is rejected
+ * (PICO_ERR_INVALID_ARG) by all three opening calls. */
 pico_status pico_gpu_reduced_opening(pico_ctx *ctx, const pico_open_batch *batches, uint32_t n_batches,
                                      uint32_t log_blowup, const uint32_t *values, const uint32_t alpha[4],
                                      uint32_t log_height, uint32_t *out);

@@ -45,19 +45,20 @@ struct ReduceTerm {
   uint32_t a[4];
   uint32_t wa[4];
 };
+// One launch of k_reduce: the low coset (2^log_h rows) of the matrices of one
+// height, for up to four of its points; writes S_q (EF4) for each at row
+// rev(i) of s_out, columns s_col0 + 4q .. + 3 (rows of s_stride words).
 struct ReduceHeight {
-  uint32_t log_h;
+  uint32_t log_h;        // rows of the low coset (log)
   uint32_t n_mats;
-  uint32_t n_slots;      // distinct points at this height handled by this launch (1..4)
-  uint32_t accumulate;   // add to ro instead of overwriting
+  uint32_t n_slots;      // points handled by this launch (1..4)
+  uint32_t s_stride;
+  uint32_t s_col0;
+  uint32_t apow_len;
   const ReduceMat* mats;
   const ReduceTerm* terms;
   const uint4* apow;     // alpha^k, EF4, k < apow_len
-  uint32_t apow_len;
-  uint32_t pad;
-  const uint4* dinv[4];  // 1 / (z_slot - x_i)
-  Ext4 K[4];             // sum over (m, z_slot) of alpha^off * sum_j alpha^j p_j(z)
-  uint4* ro;
+  uint32_t* s_out;
 };
 
 // Pieces of a query record.
@@ -78,6 +79,10 @@ cudaError_t launch_open_values(int field, const OpenDesc* descs, uint32_t n_desc
                                uint32_t max_items, const uint32_t* const* dinv_tables, TwiddleTables tw,
                                uint32_t* partial, const uint32_t* scale, uint32_t* values, cudaStream_t st);
 cudaError_t launch_reduce(int field, const ReduceHeight& h, cudaStream_t st);
+// ro[k] = sum_q dinv[q][rev(k)] * (K[q] - S[k][q]) for k < 2^log_n, natural order
+// (S rows of s_stride words).
+cudaError_t launch_reduce_combine(int field, uint32_t log_n, const uint32_t* s, uint32_t s_stride, uint32_t n_slots,
+                                  const uint32_t* const* dinv, const uint32_t* K, uint32_t* ro, cudaStream_t st);
 // Bounds guard of the reduction's tile copies (synchronous read-back / clear).
 cudaError_t open_guard_fetch(GuardRecord* dst);
 cudaError_t open_guard_clear();

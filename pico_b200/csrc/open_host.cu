@@ -149,6 +149,21 @@ struct Opening {
     return r;
   }
 
+  // A point on a committed coset g * H_N makes 1/(z - x) undefined (Plonky3
+  // fails on the inversion); such a point is a base-field element with
+  // (z / g)^N = 1.
+  bool on_coset(const Ext4& z, uint32_t log_N) const {
+    if (z.c[1] | z.c[2] | z.c[3]) return false;
+    const uint32_t y = B::mul(z.c[0], B::inv(B::to_monty(F::GENERATOR)));
+    return B::pow(y, 1ull << log_N) == F::ONE;
+  }
+  // the first opened point lying on its matrix's committed coset, or -1
+  int64_t point_on_coset() const {
+    for (size_t i = 0; i < pairs.size(); i++)
+      if (on_coset(pts[pairs[i].pt], batches[pairs[i].b].commit->log_N[pairs[i].m])) return (int64_t)i;
+    return -1;
+  }
+
   void collect_points() {
     uint64_t vofs = 0;
     for (uint32_t b = 0; b < n_batches; b++) {
@@ -172,10 +187,27 @@ struct Opening {
     }
   }
 
+  // Device bytes of the reduction's S sums, their extension and its scratch
+  // (heights with points; only_height < 32: that height alone).
+  uint64_t reduce_bytes(uint32_t only_height = 32) const {
+    uint64_t t = 0;
+    for (uint32_t h = 0; h < 32; h++) {
+      if (only_height < 32 && h != only_height) continue;
+      std::vector<uint32_t> slots;
+      for (const Pair& pr : pairs)
+        if (batches[pr.b].commit->log_N[pr.m] == h && std::find(slots.begin(), slots.end(), pr.pt) == slots.end())
+          slots.push_back(pr.pt);
+      if (slots.empty()) continue;
+      const uint64_t sw = 16ull * slots.size();  // bytes per row of S
+      t += (sw << (h - log_b)) + 2 * (16ull << (h - log_b)) + (16ull << h) + (4ull << log_b) * kPwWords;
+    }
+    return t;
+  }
+
   // Footprint reserved against the context budget for phase 1.
   uint64_t dtab_bytes() const {
     uint64_t s = 0;
-    for (uint32_t l : pt_log) s += 16ull << l;
+    for (uint32_t l : pt_log) s += 16ull << (l - log_b);
     return s;
   }
 
@@ -205,9 +237,12 @@ struct Opening {
     const TwiddleTables tw = twiddles(ctx, F::ID);
     for (size_t q = 0; q < pts.size(); q++) {
       void* p;
-      if ((s = ar.get(&p, 16ull << pt_log[q]))) return s;
+      // the low coset of the tallest height it is opened at: both the opened
+      // values and the reduced openings are formed there
+      const uint32_t lq = pt_log[q] - log_b;
+      if ((s = ar.get(&p, 16ull << lq))) return s;
       dtab.push_back((uint32_t*)p);
-      if ((s = cuda_status(launch_inv_denoms(F::ID, pts[q].c, pt_log[q], tw, (uint32_t*)p, st), "inverse denominators")))
+      if ((s = cuda_status(launch_inv_denoms(F::ID, pts[q].c, lq, tw, (uint32_t*)p, st), "inverse denominators")))
         return s;
       launches++;
     }
@@ -326,14 +361,25 @@ struct Opening {
     }
     Ext4* d_apow;
     if ((s = ar.upload(&d_apow, apow))) return s;
-    // per height: launches of up to kSlotsPerLaunch distinct points
+    // per height: S_z over the low coset (launches of up to kSlotsPerLaunch
+    // points), its extension to the LDE domain, then the combination
     std::vector<ReduceMat> hmats;
     std::vector<ReduceTerm> hterms;
     struct Launch {
       ReduceHeight h;
       size_t mat0, n_mats, term0;
     };
+    struct Height {
+      uint32_t h, n_slots;
+      uint32_t* s_low;     // n x 4 n_slots, natural order
+      uint32_t* ro_low;    // n x 4, natural order
+      size_t dinv0, k0;    // into the per-height pointer / constant arrays
+    };
+    std::vector<LdeMat> ext;  // ro_low -> ro[h] (N x 4, committed order), one batch
     std::vector<Launch> plan;
+    std::vector<Height> heights;
+    std::vector<const uint32_t*> comb_dinv;
+    std::vector<Ext4> comb_k;
     std::vector<bool> present(32, false);
     for (uint32_t b = 0; b < n_batches; b++)
       for (uint32_t m = 0; m < batches[b].commit->n_mats; m++) present[batches[b].commit->log_N[m]] = true;
@@ -353,20 +399,29 @@ struct Opening {
         if ((s = cuda_status(cudaMemsetAsync(p, 0, 16ull << h, st), "zero reduced opening"))) return s;
         continue;
       }
+      const uint32_t log_n = h - log_b;
+      const uint32_t sw = 4 * (uint32_t)slots.size();  // words per row of S
+      Height H;
+      memset(&H, 0, sizeof H);
+      H.h = h;
+      H.n_slots = (uint32_t)slots.size();
+      if ((s = ar.get(&p, ((uint64_t)sw << log_n) * 4))) return s;
+      H.s_low = (uint32_t*)p;
+      H.dinv0 = comb_dinv.size();
+      H.k0 = comb_k.size();
+      for (uint32_t q : slots) comb_dinv.push_back(dtab[q]);
+      comb_k.resize(comb_k.size() + slots.size(), Ext4{{0, 0, 0, 0}});
       for (size_t s0 = 0; s0 < slots.size(); s0 += kSlotsPerLaunch) {
         const size_t ns = std::min<size_t>(kSlotsPerLaunch, slots.size() - s0);
         Launch L;
         memset(&L.h, 0, sizeof L.h);
-        L.h.log_h = h;
+        L.h.log_h = log_n;
         L.h.n_slots = (uint32_t)ns;
-        L.h.accumulate = s0 > 0;
+        L.h.s_stride = sw;
+        L.h.s_col0 = 4 * (uint32_t)s0;
+        L.h.s_out = H.s_low;
         L.h.apow = reinterpret_cast<const uint4*>(d_apow);
         L.h.apow_len = (uint32_t)T;
-        L.h.ro = reinterpret_cast<uint4*>(p);
-        for (size_t q = 0; q < ns; q++) {
-          L.h.dinv[q] = reinterpret_cast<const uint4*>(dtab[slots[s0 + q]]);
-          L.h.K[q] = Ext4{{0, 0, 0, 0}};
-        }
         L.mat0 = hmats.size();
         L.term0 = hterms.size();
         // matrices of this height with a term in these slots, transcript order
@@ -391,7 +446,8 @@ struct Opening {
                 T.wa[l] = l ? B::mul(T.a[l], Wm) : 0u;
               }
               terms.push_back(T);
-              L.h.K[sl] = E::add(L.h.K[sl], E::mul(apow[off[k]], rys[k]));
+              Ext4& K = comb_k[H.k0 + s0 + sl];
+              K = E::add(K, E::mul(apow[off[k]], rys[k]));
             }
             if (!terms.empty()) {
               ReduceMat R;
@@ -411,7 +467,7 @@ struct Opening {
                 hterms.insert(hterms.end(), terms.begin(), terms.end());
               }
               hmats.push_back(R);
-              reduce_cells += (uint64_t)R.w << h;
+              reduce_cells += (uint64_t)R.w << log_n;
             }
           }
           i = j;
@@ -420,15 +476,57 @@ struct Opening {
         L.h.n_mats = (uint32_t)L.n_mats;
         plan.push_back(L);
       }
+      // extension of ro from the low coset g*H_n to g*H_N: evaluations of
+      // ro(g y) on H_n -> on H_N (shift 1), committed (bit-reversed) rows
+      if ((s = ar.get(&p, 16ull << log_n))) return s;
+      H.ro_low = (uint32_t*)p;
+      LdeMat X;
+      memset(&X, 0, sizeof X);
+      X.log_n = log_n;
+      X.log_b = log_b;
+      X.w = 4;
+      plan_lde_tiling(X, ctx->lde_split[F::ID][log_n]);
+      X.in = H.ro_low;
+      X.out = ro[h];
+      if (X.log_n1) {
+        if ((s = ar.get(&p, 16ull << log_n))) return s;
+        X.t1 = (uint32_t*)p;
+        if ((s = ar.get(&p, 16ull << h))) return s;
+        X.t2 = (uint32_t*)p;
+      }
+      if ((s = ar.get(&p, ((uint64_t)1 << log_b) * kPwWords * 4))) return s;
+      X.pw = (uint32_t*)p;
+      X.shift = F::ONE;
+      ext.push_back(X);
+      heights.push_back(H);
     }
     ReduceMat* d_mats;
     ReduceTerm* d_terms;
-    if ((s = ar.upload(&d_mats, hmats)) || (s = ar.upload(&d_terms, hterms))) return s;
+    const uint32_t** d_dinv;
+    Ext4* d_k;
+    if ((s = ar.upload(&d_mats, hmats)) || (s = ar.upload(&d_terms, hterms)) || (s = ar.upload(&d_dinv, comb_dinv)) ||
+        (s = ar.upload(&d_k, comb_k)))
+      return s;
     for (Launch& L : plan) {
       L.h.mats = d_mats + L.mat0;
       L.h.terms = d_terms + L.term0;
       if ((s = cuda_status(launch_reduce(F::ID, L.h, st), "reduced opening"))) return s;
       launches++;
+    }
+    for (Height& H : heights) {
+      if ((s = cuda_status(launch_reduce_combine(F::ID, H.h - log_b, H.s_low, 4 * H.n_slots, H.n_slots,
+                                                 d_dinv + H.dinv0, reinterpret_cast<const uint32_t*>(d_k + H.k0),
+                                                 H.ro_low, st),
+                           "reduced opening combination")))
+        return s;
+      launches++;
+    }
+    if (!ext.empty()) {
+      uint64_t nl = 0;
+      if ((s = cuda_status(launch_lde(F::ID, ext.data(), (uint32_t)ext.size(), twiddles(ctx, F::ID), st, &nl),
+                           "reduced opening extension")))
+        return s;
+      launches += (uint32_t)nl;
     }
     if (cells) *cells = reduce_cells;
     return PICO_OK;
@@ -474,10 +572,14 @@ pico_status pcs_open_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_t n
   const auto t0 = std::chrono::steady_clock::now();
   Opening<F> O{ctx, batches, n_batches, fp->log_blowup, sh};
   O.collect_points();
+  if (O.point_on_coset() >= 0) {
+    set_error("open: an opening point lies on the committed coset of its matrix");
+    return PICO_ERR_INVALID_ARG;
+  }
   const uint32_t log_max = sh.log_max, R = sh.rounds, nq = fp->num_queries;
   const uint64_t qw = sh.query_words;
   // footprint: tables, values, reduced openings, FRI codewords and trees, queries
-  uint64_t need = O.dtab_bytes() + sh.value_words * 8 + (uint64_t)nq * qw * 4 + (1u << 20);
+  uint64_t need = O.dtab_bytes() + O.reduce_bytes() + sh.value_words * 8 + (uint64_t)nq * qw * 4 + (1u << 20);
   for (uint32_t h = 0; h <= log_max; h++) need += 16ull << h;  // reduced openings (upper bound)
   for (uint32_t r = 1; r <= R; r++) need += 16ull << (log_max - r);
   for (uint32_t r = 0; r < R; r++) need += ((2ull << (log_max - r - 1)) - 1) * 32;
@@ -680,6 +782,10 @@ pico_status open_values_t(pico_ctx* ctx, const pico_open_batch* batches, uint32_
                           const Shape& sh, uint32_t* values) {
   Opening<F> O{ctx, batches, n_batches, log_b, sh};
   O.collect_points();
+  if (O.point_on_coset() >= 0) {
+    set_error("open_values: an opening point lies on the committed coset of its matrix");
+    return PICO_ERR_INVALID_ARG;
+  }
   O.begin();
   if (!O.reserve(O.dtab_bytes() + sh.value_words * 8 + (1u << 20))) return PICO_ERR_OUT_OF_MEMORY;
   auto run = [&]() -> pico_status {
@@ -705,8 +811,13 @@ pico_status reduced_opening_t(pico_ctx* ctx, const pico_open_batch* batches, uin
                               uint32_t* out) {
   Opening<F> O{ctx, batches, n_batches, log_b, sh};
   O.collect_points();
+  if (O.point_on_coset() >= 0) {
+    set_error("reduced_opening: an opening point lies on the committed coset of its matrix");
+    return PICO_ERR_INVALID_ARG;
+  }
   O.begin();
-  if (!O.reserve(O.dtab_bytes() + (16ull << log_height) + (1u << 20))) return PICO_ERR_OUT_OF_MEMORY;
+  if (!O.reserve(O.dtab_bytes() + O.reduce_bytes(log_height) + (16ull << log_height) + (1u << 20)))
+    return PICO_ERR_OUT_OF_MEMORY;
   auto run = [&]() -> pico_status {
     pico_status s;
     if ((s = O.make_dtabs())) return s;
@@ -721,8 +832,10 @@ pico_status reduced_opening_t(pico_ctx* ctx, const pico_open_batch* batches, uin
                        "reduced opening");
   };
   pico_status s = run();
+  if (!s) s = guard_enqueue(ctx, O.slot, O.st);
   const cudaError_t e = cudaStreamSynchronize(O.st);
   if (!s) s = cuda_status(e, "reduced_opening");
+  if (!s) s = guard_verdict(ctx, O.slot);
   if (!s) s = open_guard_verdict();
   O.end();
   return s;

@@ -7,9 +7,13 @@
 //                    sum_k w_n^k / (z - g w_n^k) * y_k over each matrix's low
 //                    coset (Plonky3's interpolate_coset): per-block partial sums
 //   k_open_finalize  sums the partials and applies the scale
-//   k_reduce         the reduced opening of one height:
-//                    ro[i] = sum_z d_z[i] * (K_z - sum_(m,z) alpha^off(m,z) r_m[i]),
-//                    r_m[i] = sum_j alpha^j M[i][j], K_z = sum alpha^off * r(p(z))
+//   k_reduce         per point z of a height, over the low coset only (the
+//                    first n committed rows): S_z[i] = sum_(m,z) alpha^off(m,z) r_m[i],
+//                    r_m[i] = sum_j alpha^j M[i][j]
+//   k_reduce_combine the reduced opening on the low coset,
+//                    ro = sum_z (K_z - S_z) / (z - x), K_z = sum alpha^off * sum_j
+//                    alpha^j p_j(z) = S_z(z): a polynomial of degree < n, so the
+//                    ordinary LDE kernels extend it to the committed rows
 //   k_gather_queries the query records (rows and Merkle paths)
 //
 // Sums of products of field elements are accumulated lazily: a product of two
@@ -480,10 +484,7 @@ __device__ __forceinline__ void lazy_row_flat(uint64_t t[4], const uint32_t* til
 // banks; the alpha powers are read by all lanes at the same address.
 template <class F, int NS>
 __global__ void __launch_bounds__(32 * kReduceWarps, 5) k_reduce(ReduceHeight h) {
-  using B = Fp<F>;
-  using E = Ef<F>;
   using L = Lazy<F>;
-  constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
   __shared__ __align__(16) uint32_t tiles[kReduceWarps][2][kTileBufWords];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t N = 1ull << h.log_h;
@@ -550,22 +551,62 @@ __global__ void __launch_bounds__(32 * kReduceWarps, 5) k_reduce(ReduceHeight h)
     buf ^= 1;
   }
   if (lane >= rows) return;
-  // ro[i] (+)= sum_q d_q[i] * (K_q - S_q)
-  uint64_t o[4] = {0, 0, 0, 0};
+  // S_q at this row, stored at its natural position rev(i) (the low coset
+  // holds the evaluations at g w_n^rev(i))
+  uint32_t* so = h.s_out + bitrev64(i, (int)h.log_h) * h.s_stride + h.s_col0;
 #pragma unroll
   for (int q = 0; q < NS; q++) {
-    Ext4 u;
-#pragma unroll
-    for (int l = 0; l < 4; l++) u.c[l] = B::sub(h.K[q].c[l], L::finish(acc[q][l]));
-    const Ext4 d = ld4(h.dinv[q] + i);
+    uint4 v;
+    v.x = L::finish(acc[q][0]);
+    v.y = L::finish(acc[q][1]);
+    v.z = L::finish(acc[q][2]);
+    v.w = L::finish(acc[q][3]);
+    *reinterpret_cast<uint4*>(so + 4 * q) = v;
+  }
+}
+
+// The reduced opening on the low coset, natural order: for k < 2^log_n,
+// ro[k] = sum_q d_q[rev(k)] * (K_q - S_q[k]) (the 1/(z - x) tables are in
+// committed, bit-reversed order; S rows of s_stride words, slot q at 4q).
+// K_q = S_q(z_q), so every term is a polynomial of degree < n and so is ro:
+// its values on the whole LDE domain are its LDE.
+template <class F>
+__global__ void __launch_bounds__(256) k_reduce_combine(uint32_t log_n, const uint32_t* s, uint32_t s_stride,
+                                                        uint32_t n_slots, const uint4* const* dinv, const Ext4* K,
+                                                        uint4* ro) {
+  using B = Fp<F>;
+  using L = Lazy<F>;
+  constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= (1ull << log_n)) return;
+  const uint64_t i = bitrev64(k, (int)log_n);
+  uint64_t o[4] = {0, 0, 0, 0};
+  for (uint32_t q = 0; q < n_slots; q++) {
+    const uint4 sv = __ldg(reinterpret_cast<const uint4*>(s + k * s_stride) + q);
+    const Ext4 kq = K[q];
+    const Ext4 u{{B::sub(kq.c[0], sv.x), B::sub(kq.c[1], sv.y), B::sub(kq.c[2], sv.z), B::sub(kq.c[3], sv.w)}};
+    const Ext4 d = ld4(dinv[q] + i);
     const uint32_t wd[4] = {0, B::mul(d.c[1], Wm), B::mul(d.c[2], Wm), B::mul(d.c[3], Wm)};
     lazy_ef_mac<F>(o, d.c, wd, u);
   }
   Ext4 res;
 #pragma unroll
   for (int l = 0; l < 4; l++) res.c[l] = L::finish(o[l]);
-  if (h.accumulate) res = E::add(res, ld4(h.ro + i));
-  h.ro[i] = st4(res);
+  ro[k] = st4(res);
+}
+
+cudaError_t launch_reduce_combine(int field, uint32_t log_n, const uint32_t* s, uint32_t s_stride, uint32_t n_slots,
+                                  const uint32_t* const* dinv, const uint32_t* K, uint32_t* ro, cudaStream_t st) {
+  const uint64_t n = 1ull << log_n;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  auto d = reinterpret_cast<const uint4* const*>(dinv);
+  auto k = reinterpret_cast<const Ext4*>(K);
+  auto r = reinterpret_cast<uint4*>(ro);
+  if (field == 0)
+    k_reduce_combine<KoalaBear><<<blocks, 256, 0, st>>>(log_n, s, s_stride, n_slots, d, k, r);
+  else
+    k_reduce_combine<BabyBear><<<blocks, 256, 0, st>>>(log_n, s, s_stride, n_slots, d, k, r);
+  return cudaGetLastError();
 }
 
 template <class F>

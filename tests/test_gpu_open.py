@@ -194,8 +194,8 @@ def test_pcs_open_large_verifies(gpu, orc, f):
 
 
 def test_wrong_claim_is_rejected(gpu, orc):
-    """A point on the committed coset (z = g, where 1/(z - x_0) does not exist)
-    yields no low-degree codeword: the call fails instead of returning a proof."""
+    """A point on the committed coset (z = g, where 1/(z - x_0) does not exist;
+    Plonky3 fails on that inversion) is rejected by every opening call."""
     f, b = 1, 1
     rng = np.random.default_rng(8)
     pcs = TwoAdicFriPcs(gpu, f, b)
@@ -203,9 +203,16 @@ def test_wrong_claim_is_rejected(gpu, orc):
     _, pd = pcs.commit([(pcs.natural_domain_for_degree(32), t)])
     # z = g (the first committed x): the inverse denominator of row 0 is 1/0
     g = F.to_monty(f, np.array([F.GENERATOR[f], 0, 0, 0], np.uint32))
-    with pytest.raises(PicoError):
+    with pytest.raises(PicoError, match="coset"):
         pcs.open([(pd, [np.stack([g])])], to_gpu_challenger(new_oracle_challenger(orc, f, [])),
                  num_queries=2, proof_of_work_bits=2)
+    with pytest.raises(PicoError, match="coset"):
+        pcs.open_values([(pd, [np.stack([g])])])
+    # another point of the coset: g * w_64^5
+    x = F.to_monty(f, np.array([F.GENERATOR[f] * pow(F.two_adic_generator(f, 6), 5, F.P[f]) % F.P[f], 0, 0, 0],
+                               np.uint32))
+    with pytest.raises(PicoError, match="coset"):
+        pcs.open_values([(pd, [np.stack([x])])])
 
 
 def test_open_rejects_bad_arguments(gpu):
