@@ -651,18 +651,29 @@ def run_fri(args):
 
 
 # ---------------------------------------------------------------- serving leg
-def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30):
+# request mixes: (log2 heights low, high), widths (low, high)
+SERVING_MIXES = {
+    "survey": ((12, 21), (16, 512)),
+    # the same matrix counts with small traces (2^8 .. 2^13 rows, 8 .. 64 columns):
+    # the regime where one launch per matrix costs more than the work
+    "small": ((8, 13), (8, 64)),
+}
+
+
+def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30, mix: str = "survey"):
     """Requests of 1..40 matrices, log2 heights uniform on [12, 21], widths
-    uniform on [16, 512]; 70% KoalaBear / 30% BabyBear; log_blowup 1 or 2.
-    A request is cut to its first matrices totalling at most max_cells trace
-    cells, so that one request (with its blowup-4 LDEs and scratch) fits HBM."""
+    uniform on [16, 512] (the "small" mix: heights 2^8..2^13, widths 8..64);
+    70% KoalaBear / 30% BabyBear; log_blowup 1 or 2.  A request is cut to its
+    first matrices totalling at most max_cells trace cells, so that one
+    request (with its blowup-4 LDEs and scratch) fits HBM."""
+    (hl, hh), (wl, wh) = SERVING_MIXES[mix]
     rng = np.random.default_rng(seed)
     reqs = []
     for _ in range(n_req):
         k = int(rng.integers(1, 41))
         f = 0 if rng.random() < 0.7 else 1
         b = int(rng.integers(1, 3))
-        shapes = [(int(rng.integers(12, 22)), int(rng.integers(16, 513))) for _ in range(k)]
+        shapes = [(int(rng.integers(hl, hh + 1)), int(rng.integers(wl, wh + 1))) for _ in range(k)]
         kept, tot = [], 0
         for lh, w in shapes:
             if kept and tot + (w << lh) > max_cells:
@@ -690,7 +701,7 @@ def run_serving(args):
     from pico_b200 import fields as F
 
     dev = torch.device("cuda", 0)
-    reqs = serving_requests(args.requests)
+    reqs = serving_requests(args.requests, mix=args.mix)
     pool_cells = 1 << 30
     pools = {f: F.random_matrix_torch(f, 30, 1, 5000 + f, dev).reshape(-1) for f in (0, 1)}
 
@@ -779,7 +790,7 @@ def run_serving(args):
         "ms_per_step": total_cells / main_row["batched"]["cells_per_s"] * 1e3 / len(reqs),
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic: views into a seeded device pool",
-        "config": {"workload": "serving", "requests": len(reqs), "slots": args.slots, "offered_load": args.load,
+        "config": {"workload": "serving", "mix": args.mix, "requests": len(reqs), "slots": args.slots, "offered_load": args.load,
                    "total_cells": total_cells},
         "served": main_row["batched"],
         "served_plain": main_row["plain"],
@@ -803,6 +814,7 @@ def main():
     ap.add_argument("--load", type=float, default=0.8,
                     help="serving: offered load vs the plain form's one-at-a-time capacity")
     ap.add_argument("--slots", type=int, default=2, help="serving: requests on the device at once")
+    ap.add_argument("--mix", choices=list(SERVING_MIXES), default="survey", help="serving: request mix")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
