@@ -56,6 +56,7 @@ typedef enum { PICO_KOALABEAR = 0, PICO_BABYBEAR = 1 } pico_field;
 #define PICO_COMMIT_PLAIN 0x2u /* one matrix per launch (LDE and row hashing): the baseline form */
 #define PICO_OUTPUT_DEVICE 0x4u /* output pointers are device pointers (else host) */
 #define PICO_LDE_NATURAL_ORDER 0x8u /* coset_lde_batch: natural row order (Dft trait); default bit-reversed */
+#define PICO_P2_FOUR_LANES 0x10u /* poseidon2_permute: four threads per state (shorter latency per state) */
 
 typedef struct pico_ctx pico_ctx;
 /* Prover data of one commit: every LDE and every digest layer stays resident

@@ -34,6 +34,7 @@ PICO_INPUT_DEVICE = 0x1
 PICO_COMMIT_PLAIN = 0x2
 PICO_OUTPUT_DEVICE = 0x4
 PICO_LDE_NATURAL_ORDER = 0x8
+PICO_P2_FOUR_LANES = 0x10
 
 
 class PicoError(RuntimeError):

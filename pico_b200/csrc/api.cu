@@ -1111,7 +1111,7 @@ extern "C" pico_status pico_gpu_poseidon2_permute(pico_ctx* ctx, pico_field fiel
   pico_status s;
   const uint64_t bytes = n * 64;
   if (flags & PICO_INPUT_DEVICE) {
-    if ((s = cuda_status(launch_permute(field, states, n, st), "permute"))) return s;
+    if ((s = cuda_status(launch_permute(field, states, n, st, (flags & PICO_P2_FOUR_LANES) != 0), "permute"))) return s;
     return cuda_status(cudaStreamSynchronize(st), "permute");
   }
   if (!try_reserve(ctx, bytes)) {
@@ -1121,7 +1121,7 @@ extern "C" pico_status pico_gpu_poseidon2_permute(pico_ctx* ctx, pico_field fiel
   void* d;
   s = alloc_async(&d, bytes, st);
   if (!s) s = cuda_status(cudaMemcpyAsync(d, states, bytes, cudaMemcpyHostToDevice, st), "copy in");
-  if (!s) s = cuda_status(launch_permute(field, (uint32_t*)d, n, st), "permute");
+  if (!s) s = cuda_status(launch_permute(field, (uint32_t*)d, n, st, (flags & PICO_P2_FOUR_LANES) != 0), "permute");
   if (!s) s = cuda_status(cudaMemcpyAsync(states, d, bytes, cudaMemcpyDeviceToHost, st), "copy out");
   free_async(d, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "permute");

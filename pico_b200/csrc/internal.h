@@ -28,7 +28,10 @@ struct RowGroup {
 // --- Poseidon2 / Merkle kernels (p2_kernels.cu) -------------------------
 cudaError_t upload_p2_constants(int field, const uint32_t ext[8][16], const uint32_t* inte, int rounds_p,
                                 const uint32_t diag[16]);
-cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st);
+// four_lanes: four threads per state (the latency form).
+cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st, bool four_lanes = false);
+// Levels of at most this many nodes are compressed four threads per node.
+constexpr uint64_t kQuadMaxNodes = 16384;
 cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st,
                              unsigned block = 256);
 // Resumable row sponge: continue from state_in (nullptr: zero state) at rate

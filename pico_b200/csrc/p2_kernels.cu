@@ -211,8 +211,35 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 static inline unsigned blocks_for(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
 
-cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st) {
+// Four threads per state (the latency form).  Every thread of a launched warp
+// takes part in the shuffles; threads past the last state permute zeros and
+// store nothing.
+template <class F>
+__global__ void __launch_bounds__(256) k_permute_quad(uint32_t* states, uint64_t n) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t i = t >> 2;
+  const uint32_t q = (uint32_t)(t & 3);
+  const bool live = i < n;
+  uint32_t v[4];
+  if (live) {
+    const uint4 a = reinterpret_cast<const uint4*>(states + 16 * i)[q];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  } else {
+    v[0] = v[1] = v[2] = v[3] = 0;
+  }
+  p2_permute_quad<F>(v, q, 0xffffffffu);
+  if (live) reinterpret_cast<uint4*>(states + 16 * i)[q] = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t st, bool four_lanes) {
   if (n == 0) return cudaSuccess;
+  if (four_lanes) {
+    if (field == 0)
+      k_permute_quad<KoalaBear><<<blocks_for(4 * n, 256), 256, 0, st>>>(states, n);
+    else
+      k_permute_quad<BabyBear><<<blocks_for(4 * n, 256), 256, 0, st>>>(states, n);
+    return cudaGetLastError();
+  }
   if (field == 0)
     k_permute<KoalaBear><<<blocks_for(n, 256), 256, 0, st>>>(states, n);
   else
@@ -253,9 +280,46 @@ cudaError_t launch_absorb_rows(int field, const RowGroup& g, uint64_t rows, uint
   return cudaGetLastError();
 }
 
+// The same compression, four threads per node (levels too small to fill the
+// GPU, where one permutation's latency sets the launch's time).
+template <class F>
+__global__ void __launch_bounds__(256) k_compress_quad(const uint32_t* prev, uint32_t* next, uint64_t n,
+                                                       const uint32_t* inj) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t i = t >> 2;
+  const uint32_t q = (uint32_t)(t & 3);
+  const bool live = i < n;
+  uint32_t v[4] = {0, 0, 0, 0};
+  if (live) {
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(prev + 16 * i) + q);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+  p2_permute_quad<F>(v, q, 0xffffffffu);
+  if (inj) {
+    // compress(digest, injected digest): lanes 0, 1 keep the digest, lanes 2, 3 load the injection
+    if (q >= 2) {
+      if (live) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(inj + 8 * i) + (q - 2));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      } else {
+        v[0] = v[1] = v[2] = v[3] = 0;
+      }
+    }
+    p2_permute_quad<F>(v, q, 0xffffffffu);
+  }
+  if (live && q < 2) reinterpret_cast<uint4*>(next + 8 * i)[q] = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
 cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,
                             const uint32_t* inj_digests, cudaStream_t st) {
   if (n_next == 0) return cudaSuccess;
+  if (n_next <= kQuadMaxNodes) {
+    if (field == 0)
+      k_compress_quad<KoalaBear><<<blocks_for(4 * n_next, 256), 256, 0, st>>>(prev, next, n_next, inj_digests);
+    else
+      k_compress_quad<BabyBear><<<blocks_for(4 * n_next, 256), 256, 0, st>>>(prev, next, n_next, inj_digests);
+    return cudaGetLastError();
+  }
   if (field == 0)
     k_compress<KoalaBear><<<blocks_for(n_next, 256), 256, 0, st>>>(prev, next, n_next, inj_digests);
   else
@@ -424,18 +488,39 @@ __global__ void __launch_bounds__(256) k_tree_top(uint32_t* level, uint32_t n_in
   while (n > 1) {
     const uint32_t m = n >> 1;
     uint32_t* out = in + (size_t)n * 8;
-    uint32_t s[16];
-    if (tid < m) {
+    if (m > 64) {
+      // one thread per node
+      uint32_t st[16];
+      if (tid < m) {
 #pragma unroll
-      for (int k = 0; k < 16; k++) s[k] = buf[16 * tid + k];
-      p2_permute<F>(s);
-    }
-    __syncthreads();
-    if (tid < m) {
+        for (int k = 0; k < 16; k++) st[k] = buf[16 * tid + k];
+        p2_permute<F>(st);
+      }
+      __syncthreads();
+      if (tid < m) {
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        buf[8 * tid + k] = s[k];
-        out[8 * tid + k] = s[k];
+        for (int k = 0; k < 8; k++) {
+          buf[8 * tid + k] = st[k];
+          out[8 * tid + k] = st[k];
+        }
+      }
+    } else {
+      // four threads per node (4m <= 256): the latency form
+      const uint32_t node = tid >> 2, q = tid & 3;
+      uint32_t v[4];
+      if (tid < 4 * m) {
+        const unsigned mask = 4 * m >= 32 ? 0xffffffffu : ((1u << (4 * m)) - 1u);
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = buf[16 * node + 4 * q + k];
+        p2_permute_quad<F>(v, q, mask);
+      }
+      __syncthreads();
+      if (tid < 4 * m && q < 2) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          buf[8 * node + 4 * q + k] = v[k];
+          out[8 * node + 4 * q + k] = v[k];
+        }
       }
     }
     __syncthreads();

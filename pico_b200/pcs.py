@@ -237,9 +237,12 @@ class Poseidon2:
     def __init__(self, ctx: GpuContext, field):
         self.ctx, self.field = ctx, F.field_id(field)
 
-    def permute(self, states):
-        """In place on (n, 16) states (host numpy or CUDA tensor)."""
+    def permute(self, states, four_lanes: bool = False):
+        """In place on (n, 16) states (host numpy or CUDA tensor); four_lanes:
+        four threads per state (the latency form)."""
         flags = abi.PICO_INPUT_DEVICE if _is_device(states) else 0
+        if four_lanes:
+            flags |= abi.PICO_P2_FOUR_LANES
         abi.check(self.ctx.lib.pico_gpu_poseidon2_permute(self.ctx.handle, self.field, _ptr(states),
                                                           states.shape[0], flags))
         return states

@@ -43,6 +43,11 @@ def test_permute_kat_and_random(gpu, orc, golden, f):
     d = to_dev(st.copy())
     Poseidon2(gpu, f).permute(d)
     assert (d.cpu().numpy().view(np.uint32) == want).all()
+    # the four-lane form, with a state count that leaves a partial warp
+    for n in (1000, 7, 1):
+        got = st[:n].copy()
+        Poseidon2(gpu, f).permute(got, four_lanes=True)
+        assert (got == want[:n]).all(), n
 
 
 # ---------------------------------------------------------------- coset LDE
