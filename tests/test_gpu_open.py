@@ -224,3 +224,43 @@ def test_open_rejects_bad_arguments(gpu):
     with pytest.raises(PicoError):
         pcs.open([(pd, [np.zeros((0, 4), np.uint32)])], to_gpu_challenger(None), num_queries=1,
                  proof_of_work_bits=30)
+
+
+def test_concurrent_commits_and_openings(gpu, orc):
+    """The ABI is thread-safe (the prover commits from rayon workers): four host
+    threads each commit and open their own batch at once on one context; every
+    result equals the same work done one call at a time."""
+    import threading
+
+    f, b = 0, 1
+    jobs = []
+    for t in range(4):
+        rng = np.random.default_rng(300 + t)
+        shapes = [[(10 - t, 5 + t), (8, 3), (9 - (t % 2), 17)]]
+        jobs.append((shapes, points_mixed(rng, f), 4000 + 10 * t))
+
+    def run(shapes, fn, seed):
+        pcs, rounds, _ = setup(gpu, orc, f, b, shapes, fn, seed, oracle=False)
+        got = pcs.open(rounds, to_gpu_challenger(None), num_queries=6, proof_of_work_bits=6)
+        return rounds[0][0].root.copy(), got
+
+    want = [run(*j) for j in jobs]
+    got = [None] * len(jobs)
+    errors = []
+
+    def worker(k):
+        try:
+            got[k] = run(*jobs[k])
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(len(jobs))]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
+    for (r1, p1), (r2, p2) in zip(want, got):
+        assert np.array_equal(r1, r2)
+        for key in ("values", "roots", "final", "indices", "queries"):
+            assert np.array_equal(p1[key], p2[key]), key
