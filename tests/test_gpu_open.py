@@ -68,8 +68,8 @@ def check_proof(orc, f, b, obatches, nq, pow_bits, pr, ch0):
 
 
 SHAPES = {
-    # mixed heights, a low coset above one block (2^12 rows), narrow and wide (> 256 columns) matrices
-    "mixed": [[(6, 4), (3, 3), (6, 1), (2, 6)], [(12, 3), (5, 300)], [(7, 2)], [(1, 2), (4, 1)]],
+    # mixed heights, a low coset above one block (2^12 rows), narrow and wide (> 256 and > 512 columns) matrices
+    "mixed": [[(6, 4), (3, 3), (6, 1), (2, 6)], [(12, 3), (5, 300), (4, 600), (3, 513)], [(7, 2)], [(1, 2), (4, 1)]],
     "single": [[(9, 17)]],
 }
 
