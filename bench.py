@@ -358,6 +358,8 @@ def run_gpu(args, rank, world, local):
     hbm_peak, hbm_kind = peaks()
     lde_alg_bytes = 4 * sum(w * ((1 << lh) + (1 << (lh + b))) for lh, w in shapes)
     lde_ach = lde_alg_bytes / (lde_only_ms / 1e3) / 1e9 if lde_only_ms else None
+    lde_modmuls = sum(w * (((1 << lh) // 2) * lh * (1 + (1 << b)) + ((1 << lh) << b)) for lh, w in shapes)
+    lde_imad = lde_modmuls * IMAD_PER_MODMUL / (lde_only_ms / 1e3) / 1e12 if lde_only_ms else None
     result = {
         "metric": METRIC,
         "value": value,
@@ -412,6 +414,20 @@ def run_gpu(args, rank, world, local):
             "algorithmic_bytes": lde_alg_bytes,
             "ms": lde_only_ms,
             "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback",
+        },
+        # the same LDE time against the integer-multiply peak: algorithmic Montgomery
+        # products per column = twiddle products of the inverse and 2^b forward
+        # transforms, (n/2) log2 n each, plus the n 2^b coset scalings
+        "roofline_lde_imad": None if not lde_only_ms else {
+            "kernel": "LDE kernels, timed alone (as roofline_lde)",
+            "bound": "imad",
+            "achieved": lde_imad,
+            "peak": imad_peak,
+            "unit": "Tops/s",
+            "frac": lde_imad / imad_peak,
+            "modmuls": lde_modmuls,
+            "note": f"achieved = {IMAD_PER_MODMUL} IMAD x algorithmic Montgomery products / LDE time; the kernels "
+                    f"also spend issue slots on modular additions, shared-memory traffic and index arithmetic",
         },
         "phases_ms": {k: float(np.mean([s[k] for s in stats])) for k in ("lde_ms", "leaves_ms", "tree_ms", "total_ms")},
         "e2e": e2e,
