@@ -669,14 +669,15 @@ def run_fri(args):
 # ---------------------------------------------------------------- serving leg
 # request mixes: (log2 heights low, high), widths (low, high)
 SERVING_MIXES = {
-    "survey": ((12, 21), (16, 512)),
+    # traces of 2^12 .. 2^21 rows and 16 .. 512 columns
+    "prover": ((12, 21), (16, 512)),
     # the same matrix counts with small traces (2^8 .. 2^13 rows, 8 .. 64 columns):
     # the regime where one launch per matrix costs more than the work
     "small": ((8, 13), (8, 64)),
 }
 
 
-def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30, mix: str = "survey"):
+def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30, mix: str = "prover"):
     """Requests of 1..40 matrices, log2 heights uniform on [12, 21], widths
     uniform on [16, 512] (the "small" mix: heights 2^8..2^13, widths 8..64);
     70% KoalaBear / 30% BabyBear; log_blowup 1 or 2.  A request is cut to its
@@ -830,7 +831,7 @@ def main():
     ap.add_argument("--load", type=float, default=0.8,
                     help="serving: offered load vs the plain form's one-at-a-time capacity")
     ap.add_argument("--slots", type=int, default=2, help="serving: requests on the device at once")
-    ap.add_argument("--mix", choices=list(SERVING_MIXES), default="survey", help="serving: request mix")
+    ap.add_argument("--mix", choices=list(SERVING_MIXES), default="prover", help="serving: request mix")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
