@@ -13,6 +13,7 @@
 #include "field.cuh"
 #include "internal.h"
 #include "open.h"
+#include "p2_layers.cuh"
 #include "runtime.h"
 #include "serving.h"
 
@@ -93,40 +94,19 @@ template <class F>
 struct HostP2 {
   uint32_t ext[8][16], inte[24], diag[16];
   HostP2() { host_p2_constants<F>(ext, inte, diag); }
-  static uint32_t sbox(uint32_t x) {
-    using B = Fp<F>;
-    const uint32_t x2 = B::mul(x, x);
-    if (F::SBOX == 3) return B::mul(x2, x);
-    return B::mul(B::mul(x2, x2), B::mul(x2, x));  // x^7
-  }
-  static void external(uint32_t* s) {
-    using B = Fp<F>;
-    for (int i = 0; i < 16; i += 4) {
-      // [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]]
-      const uint32_t a = s[i], b = s[i + 1], c = s[i + 2], d = s[i + 3];
-      const uint32_t sum = B::add(B::add(a, b), B::add(c, d));
-      s[i] = B::add(sum, B::add(a, B::dbl(b)));
-      s[i + 1] = B::add(sum, B::add(b, B::dbl(c)));
-      s[i + 2] = B::add(sum, B::add(c, B::dbl(d)));
-      s[i + 3] = B::add(sum, B::add(d, B::dbl(a)));
-    }
-    uint32_t col[4];
-    for (int k = 0; k < 4; k++) col[k] = B::add(B::add(s[k], s[4 + k]), B::add(s[8 + k], s[12 + k]));
-    for (int i = 0; i < 16; i++) s[i] = B::add(s[i], col[i & 3]);
-  }
+  // The device permutation's rounds (p2_layers.cuh) with the constants in
+  // host memory.
   void permute(uint32_t* s) const {
     using B = Fp<F>;
-    external(s);
+    p2_external<F>(s);
     for (int r = 0; r < 8; r++) {
       if (r == 4)
         for (int q = 0; q < F::ROUNDS_P; q++) {
-          s[0] = sbox(B::add(s[0], inte[q]));
-          uint32_t sum = 0;
-          for (int i = 0; i < 16; i++) sum = B::add(sum, s[i]);
-          for (int i = 0; i < 16; i++) s[i] = B::add(B::mul(s[i], diag[i]), sum);
+          s[0] = p2_sbox<F>(B::add(s[0], inte[q]));
+          p2_internal_v2<F>(s, diag);
         }
-      for (int j = 0; j < 16; j++) s[j] = sbox(B::add(s[j], ext[r][j]));
-      external(s);
+      for (int j = 0; j < 16; j++) s[j] = p2_sbox<F>(B::add(s[j], ext[r][j]));
+      p2_external<F>(s);
     }
   }
 };
