@@ -115,6 +115,17 @@ typedef struct {
   uint32_t out_len;
 } pico_challenger;
 
+/* ---- DuplexChallenger on the host --------------------------------------
+ * observe / sample of DuplexChallenger<F, Perm, 16, 8>
+ * (vm/src/compiler/recursion/circuit/challenger.rs:89-106 observe and sample,
+ * 223-234 duplexing), the transcript steps pico_gpu_pcs_open runs on the host,
+ * with the same Poseidon2-16.  observe absorbs n field elements (Monty form)
+ * one at a time; sample writes the next n samples (Monty form).  No device is
+ * needed.  The host permutation uses AVX-512 or AVX2 when the CPU has them;
+ * the environment variable PICO_HOST_SIMD (0 scalar, 2 at most AVX2) caps it. */
+pico_status pico_gpu_challenger_observe(pico_field field, pico_challenger *ch, const uint32_t *values, uint64_t n);
+pico_status pico_gpu_challenger_sample(pico_field field, pico_challenger *ch, uint32_t *out, uint64_t n);
+
 /* ---- context ------------------------------------------------------------ */
 pico_status pico_gpu_init(int device, const pico_config *cfg, pico_ctx **out);
 pico_status pico_gpu_shutdown(pico_ctx *ctx);

@@ -175,6 +175,8 @@ SIGNATURES = {
     ),
     "pico_gpu_open_values": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp]),
     "pico_gpu_reduced_opening": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp, _vp, _u32, _vp]),
+    "pico_gpu_challenger_observe": (C.c_int, [C.c_int, C.POINTER(Challenger), _vp, _u64]),
+    "pico_gpu_challenger_sample": (C.c_int, [C.c_int, C.POINTER(Challenger), _vp, _u64]),
 }
 
 _lib = None

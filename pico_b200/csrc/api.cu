@@ -1,6 +1,7 @@
 // C-ABI implementation: context, device memory accounting, commit planning
 // and orchestration, LDE / MMCS / permutation entry points, FRI commit phase.
 #include <cuda_runtime.h>
+#include <immintrin.h>
 
 #include <algorithm>
 #include <chrono>
@@ -111,9 +112,180 @@ struct HostP2 {
   }
 };
 
+// The same permutation with the 16-word state in one AVX-512 register (used
+// when the host CPU has AVX-512F).  Montgomery products take the even and odd
+// lanes through two 32x32->64 multiplies each; the 4x4 external blocks are
+// rotations within 128-bit lanes and the cross-block column sums rotations of
+// the 128-bit lanes; partial rounds run lane 0's S-box in scalar code while
+// the other lanes' diagonal products proceed, then add the lane total.
+#define PICO_AVX512 __attribute__((target("avx512f"), always_inline)) inline
+template <class F>
+struct HostP2Avx512 {
+  const HostP2<F>& c;
+  explicit HostP2Avx512(const HostP2<F>& consts) : c(consts) {}
+  static PICO_AVX512 __m512i add(__m512i a, __m512i b, __m512i p) {
+    const __m512i s = _mm512_add_epi32(a, b);
+    return _mm512_min_epu32(s, _mm512_sub_epi32(s, p));
+  }
+  static PICO_AVX512 __m512i mul(__m512i a, __m512i b, __m512i p, __m512i npinv) {
+    const __m512i pe = _mm512_mul_epu32(a, b);
+    const __m512i po = _mm512_mul_epu32(_mm512_srli_epi64(a, 32), _mm512_srli_epi64(b, 32));
+    const __m512i te = _mm512_add_epi64(pe, _mm512_mul_epu32(_mm512_mul_epu32(pe, npinv), p));
+    const __m512i to = _mm512_add_epi64(po, _mm512_mul_epu32(_mm512_mul_epu32(po, npinv), p));
+    const __m512i r = _mm512_mask_blend_epi32(0xAAAA, _mm512_srli_epi64(te, 32), to);
+    return _mm512_min_epu32(r, _mm512_sub_epi32(r, p));
+  }
+  static PICO_AVX512 __m512i sbox(__m512i x, __m512i p, __m512i npinv) {
+    const __m512i x2 = mul(x, x, p, npinv);
+    if (F::SBOX == 3) return mul(x2, x, p, npinv);
+    return mul(mul(x2, x2, p, npinv), mul(x2, x, p, npinv), p, npinv);
+  }
+  static PICO_AVX512 __m512i external(__m512i x, __m512i p) {
+    const __m512i r1 = _mm512_shuffle_epi32(x, (_MM_PERM_ENUM)0x39);  // lane k <- k+1 within each block
+    const __m512i r2 = _mm512_shuffle_epi32(x, (_MM_PERM_ENUM)0x4E);
+    const __m512i r3 = _mm512_shuffle_epi32(x, (_MM_PERM_ENUM)0x93);
+    const __m512i blk = add(add(x, r1, p), add(r2, r3, p), p);
+    // M4 row k: 2 x_k + 3 x_{k+1} + x_{k+2} + x_{k+3} = block sum + x_k + 2 x_{k+1}
+    const __m512i m = add(blk, add(x, add(r1, r1, p), p), p);
+    const __m512i c1 = _mm512_shuffle_i32x4(m, m, 0x39);
+    const __m512i c2 = _mm512_shuffle_i32x4(m, m, 0x4E);
+    const __m512i c3 = _mm512_shuffle_i32x4(m, m, 0x93);
+    return add(m, add(add(m, c1, p), add(c2, c3, p), p), p);
+  }
+  // Sum of all 16 lanes, in every lane.
+  static PICO_AVX512 __m512i total(__m512i x, __m512i p) {
+    __m512i t = add(x, _mm512_shuffle_i32x4(x, x, 0x4E), p);
+    t = add(t, _mm512_shuffle_i32x4(t, t, 0xB1), p);
+    t = add(t, _mm512_shuffle_epi32(t, (_MM_PERM_ENUM)0x4E), p);
+    return add(t, _mm512_shuffle_epi32(t, (_MM_PERM_ENUM)0xB1), p);
+  }
+  __attribute__((target("avx512f"))) void permute(uint32_t* st) const {
+    using B = Fp<F>;
+    const __m512i p = _mm512_set1_epi32((int)F::P);
+    const __m512i npinv = _mm512_set1_epi32((int)F::NEG_PINV);
+    const __m512i diag = _mm512_loadu_si512(c.diag);
+    __m512i x = external(_mm512_loadu_si512(st), p);
+    for (int r = 0; r < 8; r++) {
+      if (r == 4)
+        for (int q = 0; q < F::ROUNDS_P; q++) {
+          // lanes 1..15 do not depend on lane 0's S-box: their part of the
+          // total and their diagonal products run alongside it
+          const uint32_t x0 = p2_sbox<F>(B::add((uint32_t)_mm_cvtsi128_si32(_mm512_castsi512_si128(x)), c.inte[q]));
+          const __m512i rest = _mm512_mask_set1_epi32(x, 1, 0);
+          const __m512i prod = mul(rest, diag, p, npinv);
+          const __m512i sum = add(total(rest, p), _mm512_set1_epi32((int)x0), p);
+          // lane 0: D_0 = -2
+          const uint32_t y0 = B::sub((uint32_t)_mm_cvtsi128_si32(_mm512_castsi512_si128(sum)), B::dbl(x0));
+          x = _mm512_mask_set1_epi32(add(prod, sum, p), 1, (int)y0);
+        }
+      x = sbox(add(x, _mm512_loadu_si512(c.ext[r]), p), p, npinv);
+      x = external(x, p);
+    }
+    _mm512_storeu_si512(st, x);
+  }
+};
+#undef PICO_AVX512
+
+// The AVX2 form: lanes 0-7 in `lo`, 8-15 in `hi` (blocks 0, 1 and 2, 3).
+#define PICO_AVX2 __attribute__((target("avx2"), always_inline)) inline
+template <class F>
+struct HostP2Avx2 {
+  const HostP2<F>& c;
+  explicit HostP2Avx2(const HostP2<F>& consts) : c(consts) {}
+  static PICO_AVX2 __m256i add(__m256i a, __m256i b, __m256i p) {
+    const __m256i s = _mm256_add_epi32(a, b);
+    return _mm256_min_epu32(s, _mm256_sub_epi32(s, p));
+  }
+  static PICO_AVX2 __m256i mul(__m256i a, __m256i b, __m256i p, __m256i npinv) {
+    const __m256i pe = _mm256_mul_epu32(a, b);
+    const __m256i po = _mm256_mul_epu32(_mm256_srli_epi64(a, 32), _mm256_srli_epi64(b, 32));
+    const __m256i te = _mm256_add_epi64(pe, _mm256_mul_epu32(_mm256_mul_epu32(pe, npinv), p));
+    const __m256i to = _mm256_add_epi64(po, _mm256_mul_epu32(_mm256_mul_epu32(po, npinv), p));
+    const __m256i r = _mm256_blend_epi32(_mm256_srli_epi64(te, 32), to, 0xAA);
+    return _mm256_min_epu32(r, _mm256_sub_epi32(r, p));
+  }
+  static PICO_AVX2 __m256i sbox(__m256i x, __m256i p, __m256i npinv) {
+    const __m256i x2 = mul(x, x, p, npinv);
+    if (F::SBOX == 3) return mul(x2, x, p, npinv);
+    return mul(mul(x2, x2, p, npinv), mul(x2, x, p, npinv), p, npinv);
+  }
+  // M4 on each 4-lane block of one register (block sum + x_k + 2 x_{k+1}).
+  static PICO_AVX2 __m256i m4(__m256i x, __m256i p) {
+    const __m256i r1 = _mm256_shuffle_epi32(x, 0x39);
+    const __m256i blk = add(add(x, r1, p), add(_mm256_shuffle_epi32(x, 0x4E), _mm256_shuffle_epi32(x, 0x93), p), p);
+    return add(blk, add(x, add(r1, r1, p), p), p);
+  }
+  static PICO_AVX2 void external(__m256i& lo, __m256i& hi, __m256i p) {
+    lo = m4(lo, p);
+    hi = m4(hi, p);
+    __m256i col = add(lo, hi, p);
+    col = add(col, _mm256_permute2x128_si256(col, col, 0x01), p);
+    lo = add(lo, col, p);
+    hi = add(hi, col, p);
+  }
+  static PICO_AVX2 __m256i total(__m256i lo, __m256i hi, __m256i p) {
+    __m256i t = add(lo, hi, p);
+    t = add(t, _mm256_permute2x128_si256(t, t, 0x01), p);
+    t = add(t, _mm256_shuffle_epi32(t, 0x4E), p);
+    return add(t, _mm256_shuffle_epi32(t, 0xB1), p);
+  }
+  __attribute__((target("avx2"))) void permute(uint32_t* st) const {
+    using B = Fp<F>;
+    const __m256i p = _mm256_set1_epi32((int)F::P);
+    const __m256i npinv = _mm256_set1_epi32((int)F::NEG_PINV);
+    const __m256i dlo = _mm256_loadu_si256((const __m256i*)c.diag);
+    const __m256i dhi = _mm256_loadu_si256((const __m256i*)(c.diag + 8));
+    __m256i lo = _mm256_loadu_si256((const __m256i*)st), hi = _mm256_loadu_si256((const __m256i*)(st + 8));
+    external(lo, hi, p);
+    for (int r = 0; r < 8; r++) {
+      if (r == 4)
+        for (int q = 0; q < F::ROUNDS_P; q++) {
+          const uint32_t x0 = p2_sbox<F>(B::add((uint32_t)_mm_cvtsi128_si32(_mm256_castsi256_si128(lo)), c.inte[q]));
+          const __m256i rest = _mm256_blend_epi32(lo, _mm256_setzero_si256(), 0x01);
+          const __m256i plo = mul(rest, dlo, p, npinv), phi = mul(hi, dhi, p, npinv);
+          const __m256i sum = add(total(rest, hi, p), _mm256_set1_epi32((int)x0), p);
+          const uint32_t y0 = B::sub((uint32_t)_mm_cvtsi128_si32(_mm256_castsi256_si128(sum)), B::dbl(x0));
+          lo = _mm256_blend_epi32(add(plo, sum, p), _mm256_set1_epi32((int)y0), 0x01);
+          hi = add(phi, sum, p);
+        }
+      lo = sbox(add(lo, _mm256_loadu_si256((const __m256i*)c.ext[r]), p), p, npinv);
+      hi = sbox(add(hi, _mm256_loadu_si256((const __m256i*)(c.ext[r] + 8)), p), p, npinv);
+      external(lo, hi, p);
+    }
+    _mm256_storeu_si256((__m256i*)st, lo);
+    _mm256_storeu_si256((__m256i*)(st + 8), hi);
+  }
+};
+#undef PICO_AVX2
+
+// Picks the widest form the host CPU runs: PICO_HOST_SIMD=0 forces the scalar
+// form, =2 at most AVX2 (for testing the forms against each other).
+static int host_simd_level() {
+  const char* env = getenv("PICO_HOST_SIMD");
+  const int cap = env ? atoi(env) : 3;
+  if (cap >= 3 && __builtin_cpu_supports("avx512f")) return 3;
+  if (cap >= 2 && __builtin_cpu_supports("avx2")) return 2;
+  return 0;
+}
+
 void host_permute(int field, uint32_t s[16]) {
   static const HostP2<KoalaBear> kb;
   static const HostP2<BabyBear> bb;
+  static const int simd = host_simd_level();
+  if (simd == 3) {
+    if (field == 0)
+      HostP2Avx512<KoalaBear>(kb).permute(s);
+    else
+      HostP2Avx512<BabyBear>(bb).permute(s);
+    return;
+  }
+  if (simd == 2) {
+    if (field == 0)
+      HostP2Avx2<KoalaBear>(kb).permute(s);
+    else
+      HostP2Avx2<BabyBear>(bb).permute(s);
+    return;
+  }
   if (field == 0)
     kb.permute(s);
   else
@@ -156,6 +328,33 @@ static void free_async(void* p, cudaStream_t st) {
 }
 
 extern "C" uint32_t pico_gpu_abi_version(void) { return PICO_GPU_ABI_VERSION; }
+
+extern "C" pico_status pico_gpu_challenger_observe(pico_field field, pico_challenger* ch, const uint32_t* values,
+                                                   uint64_t n) {
+  if (field != PICO_KOALABEAR && field != PICO_BABYBEAR) {
+    set_error("challenger_observe: unknown field %d", (int)field);
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (!ch || (n && !values) || ch->in_len > 7 || ch->out_len > 8) {
+    set_error("challenger_observe: null argument or corrupt challenger state");
+    return PICO_ERR_INVALID_ARG;
+  }
+  for (uint64_t i = 0; i < n; i++) pico::host_observe(field, ch, values[i]);
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_challenger_sample(pico_field field, pico_challenger* ch, uint32_t* out, uint64_t n) {
+  if (field != PICO_KOALABEAR && field != PICO_BABYBEAR) {
+    set_error("challenger_sample: unknown field %d", (int)field);
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (!ch || (n && !out) || ch->in_len > 7 || ch->out_len > 8) {
+    set_error("challenger_sample: null argument or corrupt challenger state");
+    return PICO_ERR_INVALID_ARG;
+  }
+  for (uint64_t i = 0; i < n; i++) out[i] = pico::host_sample(field, ch);
+  return PICO_OK;
+}
 extern "C" const char* pico_gpu_last_error(void) { return g_err.c_str(); }
 
 extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ctx** out) {
