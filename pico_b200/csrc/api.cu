@@ -836,11 +836,12 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
 
   // ---- compute on st, one height group at a time ----
   // Shortest group first (the order host copies arrive in): its LDE, then
-  // the digests of its rows; the tallest group's rows are the leaves and come
-  // last, then the compression levels.  A chained group (host inputs, several
-  // matrices) runs matrix by matrix as each arrives: its LDE, then the
-  // absorption of its columns into the group's row states.  Each phase sits
-  // between a pair of events, so the timings add up exactly.
+  // the digests of its rows (in the batched form, one launch for all shorter
+  // groups, just before the tallest group); the tallest group's rows are the
+  // leaves and come last, then the compression levels.  A chained group (host
+  // inputs, several matrices) runs matrix by matrix as each arrives: its LDE,
+  // then the absorption of its columns into the group's row states.  Each
+  // phase sits between a pair of events, so the timings add up exactly.
   const TwiddleTables tw = twiddles(ctx, field);
   // Width-0 matrices add nothing to a row, so they get no segment.
   auto make_group = [&](uint32_t first, uint32_t last, RowGroup& g) {
@@ -882,15 +883,58 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     return cuda_status(cudaEventRecord(ph.begin, st), "event");
   };
   auto end_phase = [&]() { return cuda_status(cudaEventRecord(c->phases.back().end, st), "event"); };
+  // The batched form hashes the rows of the shorter groups (those hashed in
+  // one pass) together: each is added to `batch` after its LDE, and one
+  // launch before the tallest group computes all their digests.  A group
+  // with few rows is a few thousand short sponges, latency-bound on its own.
+  GroupBatch batch;
+  memset(&batch, 0, sizeof batch);
+  auto flush_batch = [&]() -> pico_status {
+    if (!batch.n_groups) return PICO_OK;
+    pico_status r;
+    if ((r = begin_phase(pico_commit::kRows))) return r;
+    r = cuda_status(launch_hash_groups(field, batch, st, ctx->hash_block[field]), "row hashing");
+    c->stats.launches += 1;
+    if (!r) r = end_phase();
+    memset(&batch, 0, sizeof batch);
+    return r;
+  };
+  auto add_to_batch = [&](uint32_t first, uint32_t last, uint64_t rows, uint32_t* out) -> pico_status {
+    uint32_t segs = 0;
+    for (uint32_t k = first; k < last; k++) segs += plan.mats[k].w != 0;
+    if (batch.n_groups == (uint32_t)kBatchGroups || batch.n_segs + segs > (uint32_t)kBatchSegs)
+      if (pico_status r = flush_batch()) return r;
+    const uint32_t g = batch.n_groups;
+    batch.seg_begin[g] = batch.n_segs;
+    uint32_t width = 0;
+    for (uint32_t k = first; k < last; k++) {
+      if (plan.mats[k].w == 0) continue;
+      batch.segs[batch.n_segs].ptr = leaves[k];
+      batch.segs[batch.n_segs].width = plan.mats[k].w;
+      batch.n_segs++;
+      width += plan.mats[k].w;
+    }
+    batch.seg_begin[g + 1] = batch.n_segs;
+    batch.width[g] = width;
+    batch.out[g] = out;
+    batch.row_end[g] = (g ? batch.row_end[g - 1] : 0ull) + rows;
+    batch.n_groups = g + 1;
+    return PICO_OK;
+  };
   uint32_t* layer = c->layers;
   for (uint32_t gi = G; gi-- > 0 && !s;) {
     const uint32_t first = plan.groups[gi].first, last = plan.groups[gi].second;
     const uint64_t rows = 1ull << plan.mats[first].log_N;
     uint32_t* digests = gi == 0 ? layer : inj[gi];
     const int hash_kind = gi == 0 ? pico_commit::kLeaves : pico_commit::kRows;
+    if (gi == 0 && (s = flush_batch())) break;
     if (!chained[gi]) {
       if (copy_in && (s = cuda_status(cudaStreamWaitEvent(st, arrived[last - 1], 0), "wait for inputs"))) break;
       if ((s = begin_phase(pico_commit::kLde)) || (s = lde_mats(first, last)) || (s = end_phase())) break;
+      if (gi > 0 && !plan.plain) {
+        if ((s = add_to_batch(first, last, rows, digests))) break;
+        continue;
+      }
       RowGroup g;
       make_group(first, last, g);
       if ((s = begin_phase(hash_kind))) break;
@@ -917,6 +961,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       cols += plan.mats[k].w;
     }
   }
+  if (!s) s = flush_batch();
   destroy_events();
   if (s) return s;
   if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;

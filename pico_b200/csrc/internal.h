@@ -34,6 +34,22 @@ cudaError_t launch_permute(int field, uint32_t* states, uint64_t n, cudaStream_t
 constexpr uint64_t kQuadMaxNodes = 16384;
 cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32_t* out, cudaStream_t st,
                              unsigned block = 256);
+// Row digests of several height groups in one launch.  Group g owns global
+// rows [row_end[g-1], row_end[g]) (row_end[-1] = 0), its row r is the
+// concatenation of segs[seg_begin[g] .. seg_begin[g+1]) and its digest goes to
+// out[g] + 8 r.
+constexpr int kBatchGroups = 16;
+constexpr int kBatchSegs = 128;
+struct GroupBatch {
+  uint32_t n_groups;
+  uint32_t n_segs;
+  uint64_t row_end[kBatchGroups];
+  uint32_t* out[kBatchGroups];
+  uint32_t seg_begin[kBatchGroups + 1];
+  uint32_t width[kBatchGroups];
+  RowSeg segs[kBatchSegs];
+};
+cudaError_t launch_hash_groups(int field, const GroupBatch& b, cudaStream_t st, unsigned block = 256);
 // Resumable row sponge: continue from state_in (nullptr: zero state) at rate
 // position pos0; if digest_out, finish and write 8-word digests, else store
 // the 16-word states to state_out.  Row r's state is 16 consecutive words.

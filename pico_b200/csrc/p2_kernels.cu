@@ -60,22 +60,22 @@ __device__ __forceinline__ void hash_guard_trip(unsigned long long seg, unsigned
   }
 }
 template <class F>
-__device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t s[16], uint64_t rows) {
-  const uint32_t W = g.total_width;
+__device__ __forceinline__ void hash_row_segs(const RowSeg* segs, uint32_t n_segs, uint32_t W, uint64_t r,
+                                              uint32_t s[16]) {
   uint32_t seg = 0, col = 0;
-  uint32_t segw = g.segs[0].width;
-  const uint32_t* rowp = g.segs[0].ptr + r * segw;
+  uint32_t segw = n_segs ? segs[0].width : 0u;
+  const uint32_t* rowp = n_segs ? segs[0].ptr + r * segw : nullptr;
   for (uint32_t base = 0; base < W; base += 8) {
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       if (base + j < W) {
-        while (col == segw && seg < g.n_segs) {
+        while (col == segw && seg < n_segs) {
           seg++;
           col = 0;
-          segw = seg < g.n_segs ? g.segs[seg].width : 0u;
-          rowp = g.segs[seg < g.n_segs ? seg : 0].ptr + r * segw;
+          segw = seg < n_segs ? segs[seg].width : 0u;
+          rowp = seg < n_segs ? segs[seg].ptr + r * segw : nullptr;
         }
-        if (seg >= g.n_segs) {
+        if (seg >= n_segs) {
           hash_guard_trip(seg, col);
           s[j] = 0;
         } else {
@@ -88,10 +88,38 @@ __device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t
   }
 }
 
+template <class F>
+__device__ __forceinline__ void hash_row(const RowGroup& g, uint64_t r, uint32_t s[16], uint64_t rows) {
+  (void)rows;
+  hash_row_segs<F>(g.segs, g.n_segs, g.total_width, r, s);
+}
+
 __device__ __forceinline__ void store_digest(uint32_t* out, const uint32_t s[16]) {
   uint4* o = reinterpret_cast<uint4*>(out);
   o[0] = make_uint4(s[0], s[1], s[2], s[3]);
   o[1] = make_uint4(s[4], s[5], s[6], s[7]);
+}
+
+// Row digests of several height groups, one thread per row of any group:
+// the groups' sponges, short and latency-bound when a group has few rows,
+// run side by side instead of one launch after another.
+template <class F>
+__global__ void __launch_bounds__(256, 5) k_hash_groups(const __grid_constant__ GroupBatch b) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (b.n_groups == 0 || b.n_groups > (uint32_t)kBatchGroups || t >= b.row_end[b.n_groups - 1]) return;
+  uint32_t g = 0;
+  while (g + 1 < b.n_groups && t >= b.row_end[g]) g++;
+  const uint64_t r = t - (g ? b.row_end[g - 1] : 0ull);
+  const uint32_t s0 = b.seg_begin[g], s1 = b.seg_begin[g + 1];
+  if (s1 < s0 || s1 > (uint32_t)kBatchSegs) {
+    hash_guard_trip(s0, s1);
+    return;
+  }
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = 0;
+  hash_row_segs<F>(b.segs + s0, s1 - s0, b.width[g], r, s);
+  store_digest(b.out[g] + 8 * r, s);
 }
 
 template <class F>
@@ -267,6 +295,19 @@ cudaError_t launch_hash_rows(int field, const RowGroup& g, uint64_t rows, uint32
     k_hash_rows<KoalaBear><<<blocks_for(rows, block), block, 0, st>>>(g, rows, out);
   else
     k_hash_rows<BabyBear><<<blocks_for(rows, block), block, 0, st>>>(g, rows, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hash_groups(int field, const GroupBatch& b, cudaStream_t st, unsigned block) {
+  if (b.n_groups == 0) return cudaSuccess;
+  if (b.n_groups > (uint32_t)kBatchGroups || b.n_segs > (uint32_t)kBatchSegs) return cudaErrorInvalidValue;
+  const uint64_t rows = b.row_end[b.n_groups - 1];
+  if (rows == 0) return cudaSuccess;
+  if (block < 32 || block > 256) block = 256;
+  if (field == 0)
+    k_hash_groups<KoalaBear><<<blocks_for(rows, block), block, 0, st>>>(b);
+  else
+    k_hash_groups<BabyBear><<<blocks_for(rows, block), block, 0, st>>>(b);
   return cudaGetLastError();
 }
 
