@@ -645,6 +645,9 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   }
   plan.permutations += plan.leaf_permutations + ((1ull << plan.log_max) - 1);
   scr += state_rows * 64;
+  // enqueue_commit carves both blocks into 256-byte aligned sub-buffers
+  res += 256ull * (n + 1);
+  scr += 256ull * (3ull * n + 4);
   plan.bytes_resident = res;
   plan.bytes_scratch = scr;
   return PICO_OK;
@@ -674,7 +677,6 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   c->lde.assign(n, nullptr);
   c->log_N.assign(n, 0);
   c->width.assign(n, 0);
-  c->owns.assign(n, false);
   c->bytes_resident = plan.bytes_resident;
   c->stats.cells = plan.cells;
   c->stats.lde_cells = plan.extend ? plan.lde_cells : 0;
@@ -685,33 +687,95 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     if ((s = cuda_status(cudaEventCreate(&c->ev[e]), "event"))) return s;
   if ((s = cuda_status(cudaEventRecord(c->ev[0], st), "event"))) return s;
 
-  // ---- allocations (stream-ordered on st) ----
-  std::vector<const uint32_t*> dev_in(n, nullptr);
-  std::vector<uint64_t> in_bytes(n, 0);
+  // ---- allocations: two stream-ordered blocks on st ----
+  // `arena` stays with the commit until release: the LDEs (or, for a commit
+  // without extension, the copied host inputs) and the digest layers.  The
+  // scratch block is freed after the commit: host-input staging of extended
+  // commits, power tables, four-step scratch, injected-row digests and the
+  // chained row states.  Two allocations instead of one per buffer: a
+  // stream-ordered allocation costs microseconds of host time, and a commit
+  // of many small matrices made dozens of them.
+  struct Carve {
+    uint64_t bytes = 0;
+    uint64_t take(uint64_t b) {
+      const uint64_t off = bytes;
+      bytes += (std::max<uint64_t>(b, 16) + 255) & ~255ull;  // 256-byte aligned sub-buffers
+      return off;
+    }
+  } res, scr;
+  constexpr uint64_t kNone = ~0ull;
+  // With host inputs, a group of several matrices is hashed one matrix at a
+  // time as each arrives (resumable sponge), the row states kept in `state`
+  // between matrices; its size is the largest such group's rows x 16 words.
+  // The plain form hashes matrix by matrix too (one launch per matrix).
+  auto nonzero = [&](uint32_t gi) {
+    uint32_t c = 0;
+    for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) c += plan.mats[k].w != 0;
+    return c;
+  };
+  std::vector<bool> chained(G, false);
+  uint64_t rows_max = 0;
+  for (uint32_t gi = 0; gi < G; gi++) {
+    chained[gi] = (copy_in || plan.plain) && nonzero(gi) >= 2;
+    if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
+  }
+  const uint32_t nb = 1u << plan.log_b;
+  std::vector<uint64_t> in_bytes(n, 0), off_in(n, kNone), off_out(n, kNone), off_t1(n, kNone), off_t2(n, kNone);
   for (uint32_t k = 0; k < n; k++) {
     const PlannedMat& m = plan.mats[k];
     in_bytes[k] = ((uint64_t)m.w << m.log_n) * 4;
-    if (in_bytes[k] == 0) {
-      dev_in[k] = nullptr;  // a width-0 matrix: nothing to read, on either side
-    } else if (!copy_in) {
-      dev_in[k] = m.src;
-    } else {
-      void* d;
-      if ((s = alloc_async(&d, in_bytes[k], st))) return s;
-      if (plan.extend)
-        scratch.push_back(d);
-      else
-        c->owns[m.input_idx] = true;
-      dev_in[k] = (const uint32_t*)d;
+    if (in_bytes[k] && copy_in) off_in[k] = plan.extend ? scr.take(in_bytes[k]) : res.take(in_bytes[k]);
+  }
+  uint64_t off_pw = kNone;
+  if (plan.extend) {
+    off_pw = scr.take((uint64_t)n * nb * kPwWords * 4);
+    for (uint32_t k = 0; k < n; k++) {
+      const PlannedMat& m = plan.mats[k];
+      off_out[k] = res.take(((uint64_t)m.w << m.log_N) * 4);
+      LdeMat probe;
+      memset(&probe, 0, sizeof probe);
+      probe.log_n = m.log_n;
+      plan_lde_tiling(probe, m.log_n <= kLdeMaxLogN ? ctx->lde_split[field][m.log_n] : 0u);
+      if (probe.log_n1) {
+        off_t1[k] = scr.take(((uint64_t)m.w << m.log_n) * 4);
+        off_t2[k] = scr.take(((uint64_t)m.w << m.log_N) * 4);
+      }
     }
+  }
+  const uint32_t log_max = plan.log_max;
+  const uint64_t off_layers = res.take(((2ull << log_max) - 1) * 32);
+  uint64_t inj_words = 0;
+  for (uint32_t g = 1; g < G; g++) inj_words += 8ull << plan.mats[plan.groups[g].first].log_N;
+  const uint64_t off_inj = inj_words ? scr.take(inj_words * 4) : kNone;
+  const uint64_t off_state = rows_max ? scr.take(rows_max * 64) : kNone;
+  uint8_t *arena = nullptr, *sbuf = nullptr;
+  {
+    void* d;
+    if ((s = alloc_async(&d, res.bytes, st))) return s;
+    arena = (uint8_t*)d;
+    c->arena = d;
+    if (scr.bytes) {
+      if ((s = alloc_async(&d, scr.bytes, st))) return s;
+      scratch.push_back(d);
+      sbuf = (uint8_t*)d;
+    }
+  }
+  auto in_res = [&](uint64_t off) { return (uint32_t*)(arena + off); };
+  auto in_scr = [&](uint64_t off) { return (uint32_t*)(sbuf + off); };
+  std::vector<const uint32_t*> dev_in(n, nullptr);
+  for (uint32_t k = 0; k < n; k++) {
+    const PlannedMat& m = plan.mats[k];
+    if (in_bytes[k] == 0)
+      dev_in[k] = nullptr;  // a width-0 matrix: nothing to read, on either side
+    else if (!copy_in)
+      dev_in[k] = m.src;
+    else
+      dev_in[k] = plan.extend ? in_scr(off_in[k]) : in_res(off_in[k]);
   }
   std::vector<LdeMat> hm(plan.extend ? n : 0);
   std::vector<const uint32_t*> leaves(n, nullptr);  // what the tree hashes, per planned matrix
   if (plan.extend) {
-    const uint32_t nb = 1u << plan.log_b;
-    void* pw;  // one allocation for all (matrix, coset) power tables
-    if ((s = alloc_async(&pw, (uint64_t)n * nb * kPwWords * 4, st))) return s;
-    scratch.push_back(pw);
+    uint32_t* pw = in_scr(off_pw);  // all (matrix, coset) power tables
     for (uint32_t k = 0; k < n; k++) {
       const PlannedMat& m = plan.mats[k];
       LdeMat& L = hm[k];
@@ -721,24 +785,20 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       L.log_b = plan.log_b;
       L.w = m.w;
       L.shift = m.shift % (field == 0 ? KoalaBear::P : BabyBear::P);
-      L.pw = (uint32_t*)pw + (uint64_t)k * nb * kPwWords;
+      L.pw = pw + (uint64_t)k * nb * kPwWords;
       plan_lde_tiling(L, m.log_n <= kLdeMaxLogN ? ctx->lde_split[field][m.log_n] : 0u);
-      void* out;
-      if ((s = alloc_async(&out, ((uint64_t)m.w << m.log_N) * 4, st))) return s;
-      L.out = (uint32_t*)out;
+      L.out = in_res(off_out[k]);
       c->lde[m.input_idx] = L.out;
-      c->owns[m.input_idx] = true;
       c->log_N[m.input_idx] = m.log_N;
       c->width[m.input_idx] = m.w;
       leaves[k] = L.out;
       if (L.log_n1) {
-        void *t1, *t2;
-        if ((s = alloc_async(&t1, ((uint64_t)m.w << m.log_n) * 4, st))) return s;
-        scratch.push_back(t1);
-        if ((s = alloc_async(&t2, ((uint64_t)m.w << m.log_N) * 4, st))) return s;
-        scratch.push_back(t2);
-        L.t1 = (uint32_t*)t1;
-        L.t2 = (uint32_t*)t2;
+        if (off_t1[k] == kNone || off_t2[k] == kNone) {
+          set_error("commit: four-step scratch was not planned for matrix %u", k);
+          return PICO_ERR_INVALID_ARG;
+        }
+        L.t1 = in_scr(off_t1[k]);
+        L.t2 = in_scr(off_t2[k]);
       }
     }
   } else {
@@ -750,50 +810,17 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       c->width[m.input_idx] = m.w;
     }
   }
-  const uint32_t log_max = plan.log_max;
-  void* layers;
-  if ((s = alloc_async(&layers, ((2ull << log_max) - 1) * 32, st))) return s;
-  c->layers = (uint32_t*)layers;
+  c->layers = in_res(off_layers);
   // digests of the rows of every shorter height group, injected at its level
   std::vector<uint32_t*> inj(G, nullptr);
-  {
-    uint64_t words = 0;
-    for (uint32_t g = 1; g < G; g++) words += 8ull << plan.mats[plan.groups[g].first].log_N;
-    if (words) {
-      void* d;
-      if ((s = alloc_async(&d, words * 4, st))) return s;
-      scratch.push_back(d);
-      uint64_t off = 0;
-      for (uint32_t g = 1; g < G; g++) {
-        inj[g] = (uint32_t*)d + off;
-        off += 8ull << plan.mats[plan.groups[g].first].log_N;
-      }
+  if (inj_words) {
+    uint64_t off = 0;
+    for (uint32_t g = 1; g < G; g++) {
+      inj[g] = in_scr(off_inj) + off;
+      off += 8ull << plan.mats[plan.groups[g].first].log_N;
     }
   }
-  // With host inputs, a group of several matrices is hashed one matrix at a
-  // time as each arrives (resumable sponge), the row states kept in `state`
-  // between matrices; its size is the largest such group's rows x 16 words.
-  // The plain form hashes matrix by matrix too (one launch per matrix).
-  auto nonzero = [&](uint32_t gi) {
-    uint32_t c = 0;
-    for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) c += plan.mats[k].w != 0;
-    return c;
-  };
-  std::vector<bool> chained(G, false);
-  uint32_t* state = nullptr;
-  {
-    uint64_t rows_max = 0;
-    for (uint32_t gi = 0; gi < G; gi++) {
-      chained[gi] = (copy_in || plan.plain) && nonzero(gi) >= 2;
-      if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
-    }
-    if (rows_max) {
-      void* d;
-      if ((s = alloc_async(&d, rows_max * 64, st))) return s;
-      scratch.push_back(d);
-      state = (uint32_t*)d;
-    }
-  }
+  uint32_t* state = off_state == kNone ? nullptr : in_scr(off_state);
 
   // ---- host -> device copies on cst: shortest group first, each group's
   // matrices in commit order; arrived[k] marks matrix k (and all before it) ----
@@ -1017,9 +1044,8 @@ pico_status finish_stats(pico_commit* c) {
 }
 
 void free_commit_buffers(pico_commit* c, cudaStream_t st) {
-  for (uint32_t i = 0; i < c->lde.size(); i++)
-    if (c->owns[i]) free_async(c->lde[i], st);
-  free_async(c->layers, st);
+  free_async(c->arena, st);  // LDEs, copied inputs and layers are views into it
+  c->arena = nullptr;
   c->lde.clear();
   c->layers = nullptr;
 }

@@ -120,8 +120,8 @@ struct pico_commit {
   std::vector<uint32_t*> lde;     // per input index: device LDE (bit-reversed rows)
   std::vector<uint32_t> log_N;    // per input index
   std::vector<uint32_t> width;    // per input index
-  std::vector<bool> owns;         // whether lde[i] is owned by the commit
-  uint32_t* layers = nullptr;     // all digest layers, leaves first
+  void* arena = nullptr;          // the commit's device block: owned LDEs / copied inputs and the layers
+  uint32_t* layers = nullptr;     // all digest layers, leaves first (a view into arena)
   uint64_t bytes_resident = 0;
   uint32_t root[8] = {0};
   // events (see finish_stats): compute-stream phases 0, 3, 4, copy stream 5..6,
