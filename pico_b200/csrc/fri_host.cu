@@ -95,6 +95,7 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
   uint64_t resident = 0;
   for (uint32_t r = 0; r <= R; r++) resident += (16ull << (log_n - r));
   for (uint32_t r = 0; r < R; r++) resident += ((2ull << (log_n - r - 1)) - 1) * 32;
+  resident += 256ull * (2 * R + 1);  // alignment of the views into one block
   const uint64_t small = 4096 + 16ull * (R + 1) + (16ull << log_final_len);
   if (!try_reserve(ctx, resident + small)) {
     set_error("fri_commit_phase: HBM budget exceeded");
@@ -117,31 +118,37 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
   auto run = [&]() -> pico_status {
     pico_status s;
     void* p;
-    for (uint32_t r = 0; r <= R; r++) {
-      if ((s = fri_alloc(&p, 16ull << (log_n - r), st))) return s;
-      f->codewords.push_back((uint32_t*)p);
-    }
-    for (uint32_t r = 0; r < R; r++) {
-      if ((s = fri_alloc(&p, ((2ull << (log_n - r - 1)) - 1) * 32, st))) return s;
-      f->trees.push_back((uint32_t*)p);
-    }
+    // codewords and trees: one block (views at 256-byte aligned offsets);
+    // one stream-ordered allocation per round would cost more host time than
+    // the small rounds take on the device
+    uint64_t bytes = 0;
+    std::vector<uint64_t> off_cw(R + 1), off_tree(R);
+    auto take = [&](uint64_t b) {
+      const uint64_t o = bytes;
+      bytes += (b + 255) & ~255ull;
+      return o;
+    };
+    for (uint32_t r = 0; r <= R; r++) off_cw[r] = take(16ull << (log_n - r));
+    for (uint32_t r = 0; r < R; r++) off_tree[r] = take(((2ull << (log_n - r - 1)) - 1) * 32);
+    if ((s = fri_alloc(&p, bytes, st))) return s;
+    f->arena = p;
+    for (uint32_t r = 0; r <= R; r++) f->codewords.push_back((uint32_t*)((uint8_t*)p + off_cw[r]));
+    for (uint32_t r = 0; r < R; r++) f->trees.push_back((uint32_t*)((uint8_t*)p + off_tree[r]));
     if ((s = cuda_status(cudaMemcpyAsync(f->codewords[0], codeword, 16ull << log_n,
                                          (flags & PICO_INPUT_DEVICE) ? cudaMemcpyDeviceToDevice
                                                                      : cudaMemcpyHostToDevice,
                                          st),
                          "codeword copy")))
       return s;
-    uint32_t *d_betas, *d_err, *d_final;
+    // betas, error flag, final polynomial and challenger: one scratch block
+    const uint64_t b_betas = (16ull * (R + 1) + 255) & ~255ull, b_err = 256;
+    const uint64_t b_final = ((16ull << log_final_len) + 255) & ~255ull;
+    if ((s = fri_alloc(&p, b_betas + b_err + b_final + sizeof(DevChallenger), st))) return s;
+    scratch.push_back(p);
+    uint32_t* d_betas = (uint32_t*)p;
+    uint32_t* d_err = (uint32_t*)((uint8_t*)p + b_betas);
+    uint32_t* d_final = (uint32_t*)((uint8_t*)p + b_betas + b_err);
     DevChallenger* d_ch = nullptr;
-    if ((s = fri_alloc(&p, 16ull * (R + 1), st))) return s;
-    scratch.push_back(p);
-    d_betas = (uint32_t*)p;
-    if ((s = fri_alloc(&p, 16, st))) return s;
-    scratch.push_back(p);
-    d_err = (uint32_t*)p;
-    if ((s = fri_alloc(&p, 16ull << log_final_len, st))) return s;
-    scratch.push_back(p);
-    d_final = (uint32_t*)p;
     if ((s = cuda_status(cudaMemsetAsync(d_err, 0, 4, st), "memset"))) return s;
     if (betas_in) {
       if ((s = cuda_status(cudaMemcpyAsync(d_betas, betas_in, 16ull * R, cudaMemcpyHostToDevice, st), "betas")))
@@ -149,9 +156,7 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
     }
     if (ch) {
       static_assert(sizeof(DevChallenger) == sizeof(pico_challenger), "challenger layout");
-      if ((s = fri_alloc(&p, sizeof(DevChallenger), st))) return s;
-      scratch.push_back(p);
-      d_ch = (DevChallenger*)p;
+      d_ch = (DevChallenger*)((uint8_t*)scratch.back() + b_betas + b_err + b_final);
       if ((s = cuda_status(cudaMemcpyAsync(d_ch, ch, sizeof *ch, cudaMemcpyHostToDevice, st), "challenger")))
         return s;
     }
@@ -221,8 +226,7 @@ extern "C" pico_status pico_gpu_fri_commit_phase(pico_ctx* ctx, pico_field field
   }
   if (!s && n_rounds) *n_rounds = R;
   if (s || !out) {
-    for (auto p : f->codewords) cudaFreeAsync(p, st);
-    for (auto p : f->trees) cudaFreeAsync(p, st);
+    if (f->arena) cudaFreeAsync(f->arena, st);
     cudaStreamSynchronize(st);
     unreserve(ctx, resident);
     return s;
@@ -239,8 +243,7 @@ extern "C" pico_status pico_gpu_fri_release(pico_ctx* ctx, pico_fri* f) {
   }
   cudaSetDevice(ctx->device);
   cudaStream_t st = aux_stream(ctx);
-  for (auto p : f->codewords) cudaFreeAsync(p, st);
-  for (auto p : f->trees) cudaFreeAsync(p, st);
+  if (f->arena) cudaFreeAsync(f->arena, st);
   pico_status s = cuda_status(cudaStreamSynchronize(st), "fri_release");
   unreserve(ctx, f->bytes_resident);
   delete f;

@@ -120,8 +120,8 @@ struct pico_commit {
   std::vector<uint32_t*> lde;     // per input index: device LDE (bit-reversed rows)
   std::vector<uint32_t> log_N;    // per input index
   std::vector<uint32_t> width;    // per input index
-  void* arena = nullptr;          // the commit's device block: owned LDEs / copied inputs and the layers
-  uint32_t* layers = nullptr;     // all digest layers, leaves first (a view into arena)
+  std::vector<void*> blocks;      // the commit's device allocations: owned LDEs / copied inputs, layers
+  uint32_t* layers = nullptr;     // all digest layers, leaves first (in one of the blocks)
   uint64_t bytes_resident = 0;
   uint32_t root[8] = {0};
   // events (see finish_stats): compute-stream phases 0, 3, 4, copy stream 5..6,
@@ -144,5 +144,6 @@ struct pico_fri {
   uint32_t log_n = 0, rounds = 0;
   std::vector<uint32_t*> codewords;  // round r: 2^(log_n - r) x 4
   std::vector<uint32_t*> trees;      // round r: digest layers over 2^(log_n - r - 1) leaves
+  void* arena = nullptr;             // codewords and trees are views into it
   uint64_t bytes_resident = 0;
 };
