@@ -760,7 +760,9 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   for (uint32_t g = 1; g < G; g++) inj_words += 8ull << plan.mats[plan.groups[g].first].log_N;
   const uint64_t ix_inj = inj_words ? scr.take(inj_words * 4) : kNone;
   const uint64_t ix_state = rows_max ? scr.take(rows_max * 64) : kNone;
-  const bool packed = res.bytes + scr.bytes <= kPackedCommitBytes;
+  const char* packed_env = getenv("PICO_PACKED_COMMIT_BYTES");  // tests force either form with it
+  const uint64_t packed_max = packed_env ? strtoull(packed_env, nullptr, 10) : kPackedCommitBytes;
+  const bool packed = res.bytes + scr.bytes <= packed_max;
   res.ptr.assign(res.off.size(), nullptr);
   scr.ptr.assign(scr.off.size(), nullptr);
   void* d;

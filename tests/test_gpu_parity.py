@@ -170,6 +170,28 @@ def test_autotune_keeps_parity(gpu, orc, f):
 
 
 @pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("packed_max", ["0", str(1 << 40)])
+def test_commit_allocation_forms(gpu, orc, f, packed_max, monkeypatch):
+    """A commit's buffers are two blocks (commits up to PICO_PACKED_COMMIT_BYTES)
+    or one allocation each: both forms give the oracle's LDEs, layers and root,
+    with host and with device inputs."""
+    monkeypatch.setenv("PICO_PACKED_COMMIT_BYTES", packed_max)
+    shapes = [(9, 30), (5, 3), (9, 1), (7, 64), (0, 2), (7, 5), (3, 0)]
+    for device in (False, True):
+        mats, root, pd, want_root, want_ldes, want_layers = commit_both(gpu, orc, f, shapes, 2, 1100 + f,
+                                                                        device=device)
+        assert root.tolist() == want_root.tolist()
+        for i in range(len(mats)):
+            assert (pd.lde(i) == want_ldes[i]).all()
+        off = 0
+        for lvl in range(pd.log_max_height + 1):
+            got = pd.digest_layer(lvl)
+            assert (got == want_layers[off:off + got.shape[0]]).all()
+            off += got.shape[0]
+        pd.release()
+
+
+@pytest.mark.parametrize("f", FIELDS)
 def test_commit_chained_sponge_odd_widths(gpu, orc, f):
     """Host inputs: a height group of many matrices is hashed matrix by matrix
     (resumable sponge); widths 1..17 put the matrix boundaries at every rate
