@@ -773,15 +773,24 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       (cv == &res ? c->blocks : scratch).push_back(d);
       for (size_t i = 0; i < cv->off.size(); i++) cv->ptr[i] = (uint8_t*)d + cv->off[i];
     }
-  } else {
-    // one allocation per buffer, in the order they were planned
-    for (const auto& o : order) {
+  }
+  // A large commit allocates one buffer at a time, in the order planned; the
+  // host-input buffers come first, so the copies start before the rest is
+  // allocated.
+  size_t allocated = 0;
+  auto alloc_through = [&](size_t end) -> pico_status {
+    for (; allocated < end; allocated++) {
+      const auto& o = order[allocated];
       Carve& cv = o.first == 0 ? res : scr;
-      if ((s = alloc_async(&d, cv.size[o.second], st))) return s;
+      if (pico_status r = alloc_async(&d, cv.size[o.second], st)) return r;
       (o.first == 0 ? c->blocks : scratch).push_back(d);
       cv.ptr[o.second] = (uint8_t*)d;
     }
-  }
+    return PICO_OK;
+  };
+  size_t n_inputs = 0;
+  for (uint32_t k = 0; k < n; k++) n_inputs += ix_in[k] != kNone;
+  if (!packed && (s = alloc_through(n_inputs))) return s;
   auto in_res = [&](uint64_t i) { return (uint32_t*)res.ptr[i]; };
   auto in_scr = [&](uint64_t i) { return (uint32_t*)scr.ptr[i]; };
   std::vector<const uint32_t*> dev_in(n, nullptr);
@@ -793,6 +802,50 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       dev_in[k] = m.src;
     else
       dev_in[k] = plan.extend ? in_scr(ix_in[k]) : in_res(ix_in[k]);
+  }
+
+  // ---- host -> device copies on cst: shortest group first, each group's
+  // matrices in commit order; arrived[k] marks matrix k (and all before it) ----
+  std::vector<cudaEvent_t> arrived(n, nullptr);
+  auto destroy_events = [&]() {
+    for (auto e : arrived)
+      if (e) cudaEventDestroy(e);  // released once the device has passed them
+  };
+  if ((s = cuda_status(cudaEventRecord(c->ev[5], st), "event"))) return s;
+  if (copy_in) {
+    if ((s = cuda_status(cudaStreamWaitEvent(cst, c->ev[5], 0), "copy stream wait"))) return s;
+    for (uint32_t gi = G; gi-- > 0;) {
+      for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) {
+        if (in_bytes[k] &&
+            (s = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(dev_in[k]), plan.mats[k].src, in_bytes[k],
+                                             cudaMemcpyHostToDevice, cst),
+                             "input copy"))) {
+          destroy_events();
+          return s;
+        }
+        cudaEvent_t e;
+        if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) {
+          destroy_events();
+          return s;
+        }
+        arrived[k] = e;
+        if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) {
+          destroy_events();
+          return s;
+        }
+      }
+    }
+    if ((s = cuda_status(cudaEventRecord(c->ev[6], cst), "event"))) {
+      destroy_events();
+      return s;
+    }
+  } else {
+    if ((s = cuda_status(cudaEventRecord(c->ev[6], st), "event"))) return s;
+  }
+
+  if (!packed && (s = alloc_through(order.size()))) {
+    destroy_events();
+    return s;
   }
   std::vector<LdeMat> hm(plan.extend ? n : 0);
   std::vector<const uint32_t*> leaves(n, nullptr);  // what the tree hashes, per planned matrix
@@ -843,45 +896,6 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     }
   }
   uint32_t* state = ix_state == kNone ? nullptr : in_scr(ix_state);
-
-  // ---- host -> device copies on cst: shortest group first, each group's
-  // matrices in commit order; arrived[k] marks matrix k (and all before it) ----
-  std::vector<cudaEvent_t> arrived(n, nullptr);
-  auto destroy_events = [&]() {
-    for (auto e : arrived)
-      if (e) cudaEventDestroy(e);  // released once the device has passed them
-  };
-  if ((s = cuda_status(cudaEventRecord(c->ev[5], st), "event"))) return s;
-  if (copy_in) {
-    if ((s = cuda_status(cudaStreamWaitEvent(cst, c->ev[5], 0), "copy stream wait"))) return s;
-    for (uint32_t gi = G; gi-- > 0;) {
-      for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) {
-        if (in_bytes[k] &&
-            (s = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(dev_in[k]), plan.mats[k].src, in_bytes[k],
-                                             cudaMemcpyHostToDevice, cst),
-                             "input copy"))) {
-          destroy_events();
-          return s;
-        }
-        cudaEvent_t e;
-        if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) {
-          destroy_events();
-          return s;
-        }
-        arrived[k] = e;
-        if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) {
-          destroy_events();
-          return s;
-        }
-      }
-    }
-    if ((s = cuda_status(cudaEventRecord(c->ev[6], cst), "event"))) {
-      destroy_events();
-      return s;
-    }
-  } else {
-    if ((s = cuda_status(cudaEventRecord(c->ev[6], st), "event"))) return s;
-  }
 
   // ---- compute on st, one height group at a time ----
   // Shortest group first (the order host copies arrive in): its LDE, then
