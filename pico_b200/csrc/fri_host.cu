@@ -37,10 +37,21 @@ pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& 
       if ((s = cuda_status(launch_hash_rows(field, g, leaves, trees[0], st), "FRI leaf hashing"))) return s;
       nl++;
     }
-    // wide levels one launch each, the last 512 nodes and the challenger in one block
+    // wide levels one launch each; from 2^15 nodes down, seven levels per
+    // launch (k_subtree_quad); the last <= 512 nodes and the challenger in
+    // one block
     uint32_t* layer = trees[r];
     uint64_t n = leaves;
     while (n > 512) {
+      if (n <= (1u << 15)) {
+        if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)n, st), "FRI subtree"))) return s;
+        nl++;
+        for (int l = 0; l < 7; l++) {
+          layer += n * 8;
+          n /= 2;
+        }
+        continue;
+      }
       uint32_t* next = layer + n * 8;
       if ((s = cuda_status(launch_compress(field, layer, next, n / 2, nullptr, st), "FRI compression"))) return s;
       nl++;

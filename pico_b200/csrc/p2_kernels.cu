@@ -577,6 +577,59 @@ __global__ void __launch_bounds__(256) k_tree_top(uint32_t* level, uint32_t n_in
   }
 }
 
+// Seven compression levels in one launch: CTA c reduces input nodes
+// [128 c, 128 c + 128) of a level of n_in nodes to one node, four lanes per
+// state, and writes every level it computes to the tree (level l + 1 follows
+// level l, which holds n_in >> l nodes).  n_in is a multiple of 128.  For the
+// narrow levels of a tree this replaces seven latency-bound launches.
+constexpr uint32_t kSubtreeIn = 128;
+template <class F>
+__global__ void __launch_bounds__(256) k_subtree_quad(uint32_t* level, uint32_t n_in) {
+  __shared__ uint32_t buf[kSubtreeIn * 8];
+  const uint32_t tid = threadIdx.x, c = blockIdx.x;
+  if ((uint64_t)(c + 1) * kSubtreeIn > n_in) return;  // whole chunks only (the launcher checks n_in)
+  const uint32_t* src = level + (size_t)c * kSubtreeIn * 8;
+  for (uint32_t i = tid; i < kSubtreeIn * 8; i += blockDim.x) buf[i] = src[i];
+  __syncthreads();
+  uint32_t n = kSubtreeIn;  // this CTA's nodes at the current level
+  uint32_t nl = n_in;       // the whole level's nodes
+  uint32_t* in = level;
+  while (n > 1) {
+    const uint32_t m = n >> 1;
+    uint32_t* out = in + (size_t)nl * 8;
+    const uint32_t node = tid >> 2, q = tid & 3;
+    const bool live = tid < 4 * m;
+    uint32_t v[4];
+    if (live) {
+      const unsigned mask = 4 * m >= 32 ? 0xffffffffu : ((1u << (4 * m)) - 1u);
+#pragma unroll
+      for (int k = 0; k < 4; k++) v[k] = buf[16 * node + 4 * q + k];
+      p2_permute_quad<F>(v, q, mask);
+    }
+    __syncthreads();
+    if (live && q < 2) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        buf[8 * node + 4 * q + k] = v[k];
+        out[((size_t)c * m + node) * 8 + 4 * q + k] = v[k];
+      }
+    }
+    __syncthreads();
+    in = out;
+    nl >>= 1;
+    n = m;
+  }
+}
+
+cudaError_t launch_subtree(int field, uint32_t* level, uint32_t n_in, cudaStream_t st) {
+  if (n_in < kSubtreeIn || n_in % kSubtreeIn) return cudaErrorInvalidValue;
+  if (field == 0)
+    k_subtree_quad<KoalaBear><<<n_in / kSubtreeIn, 256, 0, st>>>(level, n_in);
+  else
+    k_subtree_quad<BabyBear><<<n_in / kSubtreeIn, 256, 0, st>>>(level, n_in);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_tree_top(int field, uint32_t* level, uint32_t n_in, DevChallenger* ch, uint32_t* beta_out,
                             cudaStream_t st) {
   if (n_in == 0 || n_in > kTreeTopMax || (n_in & (n_in - 1))) return cudaErrorInvalidValue;
