@@ -1029,14 +1029,28 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   if (s) return s;
   if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;
   uint32_t next_group = 1;
-  for (uint32_t lvl = 1; lvl <= log_max; lvl++) {
-    const uint64_t len = 1ull << (log_max - lvl);
+  for (uint32_t lvl = 1; lvl <= log_max;) {
+    const uint64_t len = 1ull << (log_max - lvl);  // nodes of the level being made
+    if (2 * len <= (1u << 15) && 2 * len >= kSubtreeIn) {
+      // the narrow levels seven at a time (k_subtree_quad), with the injected
+      // rows of the groups whose heights they meet
+      SubtreeInj si{};
+      for (uint32_t l = 0; l < 7; l++)
+        if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - (lvl + l))
+          si.digests[l] = inj[next_group++];
+      if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)(2 * len), si, st), "compression"))) return s;
+      c->stats.launches += 1;
+      for (uint32_t l = 0; l < 7; l++) layer += ((2 * len) >> l) * 8;
+      lvl += 7;
+      continue;
+    }
     uint32_t* next = layer + (2 * len) * 8;
     const uint32_t* d = nullptr;
     if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - lvl) d = inj[next_group++];
     if ((s = cuda_status(launch_compress(field, layer, next, len, d, st), "compression"))) return s;
     c->stats.launches += 1;
     layer = next;
+    lvl++;
   }
   if ((s = cuda_status(cudaEventRecord(c->ev[4], st), "event"))) return s;
   if (root_host)

@@ -44,7 +44,7 @@ pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& 
     uint64_t n = leaves;
     while (n > 512) {
       if (n <= (1u << 15)) {
-        if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)n, st), "FRI subtree"))) return s;
+        if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)n, SubtreeInj{}, st), "FRI subtree"))) return s;
         nl++;
         for (int l = 0; l < 7; l++) {
           layer += n * 8;

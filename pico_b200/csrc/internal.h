@@ -57,7 +57,11 @@ cudaError_t launch_absorb_rows(int field, const RowGroup& g, uint64_t rows, uint
                                uint32_t* state_out, uint32_t* digest_out, cudaStream_t st, unsigned block = 256);
 // Seven levels at once: a level of n_in nodes (a multiple of 128) down to
 // n_in / 128, every level written after the previous one (tree layout).
-cudaError_t launch_subtree(int field, uint32_t* level, uint32_t n_in, cudaStream_t st);
+constexpr uint32_t kSubtreeIn = 128;  // input nodes per CTA (seven levels down to one)
+struct SubtreeInj {
+  const uint32_t* digests[7];  // per computed level (nullptr: none), 8 words per node
+};
+cudaError_t launch_subtree(int field, uint32_t* level, uint32_t n_in, const SubtreeInj& inj, cudaStream_t st);
 // next[i] = compress(prev[2i], prev[2i+1]); if inj_digests != null:
 // next[i] = compress(next[i], inj_digests[i]) (8 words per digest).
 cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uint64_t n_next,

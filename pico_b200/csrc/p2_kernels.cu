@@ -580,11 +580,13 @@ __global__ void __launch_bounds__(256) k_tree_top(uint32_t* level, uint32_t n_in
 // Seven compression levels in one launch: CTA c reduces input nodes
 // [128 c, 128 c + 128) of a level of n_in nodes to one node, four lanes per
 // state, and writes every level it computes to the tree (level l + 1 follows
-// level l, which holds n_in >> l nodes).  n_in is a multiple of 128.  For the
-// narrow levels of a tree this replaces seven latency-bound launches.
-constexpr uint32_t kSubtreeIn = 128;
+// level l, which holds n_in >> l nodes).  n_in is a multiple of 128.  Where
+// inj.digests[l] is set, node i of computed level l is compressed once more
+// with digest i of it (a commit's injected rows).  For the narrow levels of a
+// tree this replaces seven latency-bound launches.
 template <class F>
-__global__ void __launch_bounds__(256) k_subtree_quad(uint32_t* level, uint32_t n_in) {
+__global__ void __launch_bounds__(256) k_subtree_quad(uint32_t* level, uint32_t n_in,
+                                                      const __grid_constant__ SubtreeInj inj) {
   __shared__ uint32_t buf[kSubtreeIn * 8];
   const uint32_t tid = threadIdx.x, c = blockIdx.x;
   if ((uint64_t)(c + 1) * kSubtreeIn > n_in) return;  // whole chunks only (the launcher checks n_in)
@@ -594,17 +596,27 @@ __global__ void __launch_bounds__(256) k_subtree_quad(uint32_t* level, uint32_t 
   uint32_t n = kSubtreeIn;  // this CTA's nodes at the current level
   uint32_t nl = n_in;       // the whole level's nodes
   uint32_t* in = level;
+  uint32_t lvl = 0;         // levels computed so far
   while (n > 1) {
     const uint32_t m = n >> 1;
     uint32_t* out = in + (size_t)nl * 8;
     const uint32_t node = tid >> 2, q = tid & 3;
     const bool live = tid < 4 * m;
     uint32_t v[4];
+    const uint32_t* d = inj.digests[lvl];
     if (live) {
       const unsigned mask = 4 * m >= 32 ? 0xffffffffu : ((1u << (4 * m)) - 1u);
 #pragma unroll
       for (int k = 0; k < 4; k++) v[k] = buf[16 * node + 4 * q + k];
       p2_permute_quad<F>(v, q, mask);
+      if (d) {
+        // compress(node, injected digest): lanes 2, 3 load the injection
+        if (q >= 2) {
+          const uint4 a = __ldg(reinterpret_cast<const uint4*>(d + ((size_t)c * m + node) * 8) + (q - 2));
+          v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        }
+        p2_permute_quad<F>(v, q, mask);
+      }
     }
     __syncthreads();
     if (live && q < 2) {
@@ -618,15 +630,16 @@ __global__ void __launch_bounds__(256) k_subtree_quad(uint32_t* level, uint32_t 
     in = out;
     nl >>= 1;
     n = m;
+    lvl++;
   }
 }
 
-cudaError_t launch_subtree(int field, uint32_t* level, uint32_t n_in, cudaStream_t st) {
+cudaError_t launch_subtree(int field, uint32_t* level, uint32_t n_in, const SubtreeInj& inj, cudaStream_t st) {
   if (n_in < kSubtreeIn || n_in % kSubtreeIn) return cudaErrorInvalidValue;
   if (field == 0)
-    k_subtree_quad<KoalaBear><<<n_in / kSubtreeIn, 256, 0, st>>>(level, n_in);
+    k_subtree_quad<KoalaBear><<<n_in / kSubtreeIn, 256, 0, st>>>(level, n_in, inj);
   else
-    k_subtree_quad<BabyBear><<<n_in / kSubtreeIn, 256, 0, st>>>(level, n_in);
+    k_subtree_quad<BabyBear><<<n_in / kSubtreeIn, 256, 0, st>>>(level, n_in, inj);
   return cudaGetLastError();
 }
 
