@@ -192,6 +192,22 @@ def test_commit_allocation_forms(gpu, orc, f, packed_max, monkeypatch):
 
 
 @pytest.mark.parametrize("f", FIELDS)
+def test_commit_many_height_groups(gpu, orc, f):
+    """Twenty height groups: the batched form hashes the shorter groups' rows
+    in launches of at most 16 groups, so this commit needs two; root and every
+    layer must match the oracle."""
+    shapes = [(h, 1 + (h * 7) % 5) for h in range(19, -1, -1)]
+    mats, root, pd, want_root, want_ldes, want_layers = commit_both(gpu, orc, f, shapes, 1, 1300 + f, device=True)
+    assert root.tolist() == want_root.tolist()
+    off = 0
+    for lvl in range(pd.log_max_height + 1):
+        got = pd.digest_layer(lvl)
+        assert (got == want_layers[off:off + got.shape[0]]).all()
+        off += got.shape[0]
+    pd.release()
+
+
+@pytest.mark.parametrize("f", FIELDS)
 def test_commit_chained_sponge_odd_widths(gpu, orc, f):
     """Host inputs: a height group of many matrices is hashed matrix by matrix
     (resumable sponge); widths 1..17 put the matrix boundaries at every rate
