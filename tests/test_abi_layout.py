@@ -61,3 +61,26 @@ def test_struct_layouts_match_header(tmp_path):
         for fname, _ in cls._fields_:
             got[fname] = getattr(cls, fname).offset
         assert got == want[cname], (py, got, want[cname])
+
+
+def header_prototypes() -> dict:
+    """name -> number of parameters, from the declarations in the header."""
+    import re
+
+    text = (ROOT / "include" / "pico_gpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(pico_gpu_\w+)\s*\(([^;{]*?)\)\s*;", text):
+        args = " ".join(m.group(2).split())
+        protos[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return protos
+
+
+def test_binding_argument_counts_match_header():
+    from pico_b200 import abi
+
+    protos = header_prototypes()
+    assert len(protos) >= 30
+    assert set(protos) == set(abi.SIGNATURES)
+    for name, n in protos.items():
+        assert len(abi.SIGNATURES[name][1]) == n, (name, n, len(abi.SIGNATURES[name][1]))
