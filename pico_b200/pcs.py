@@ -146,7 +146,8 @@ class ProverData:
         return out
 
     def evaluations_on_domain(self, i: int, log_domain: int, out=None):
-        """Pcs::get_evaluations_on_domain for g * H_(2^log_domain): natural row order."""
+        """Pcs::get_evaluations_on_domain for g * H_(2^log_domain): natural row order
+        (vm/src/machine/prover.rs:469-489)."""
         _, w = self.lde_shape(i)
         if out is None:
             out = np.zeros((1 << log_domain, w), dtype=np.uint32)
@@ -166,7 +167,8 @@ class ProverData:
 
 
 class MerkleTreeMmcs:
-    """MerkleTreeMmcs<_, _, PaddingFreeSponge<Perm,16,8,8>, TruncatedPermutation<Perm,2,8,16>, 8>."""
+    """MerkleTreeMmcs<_, _, PaddingFreeSponge<Perm,16,8,8>, TruncatedPermutation<Perm,2,8,16>, 8>
+    (kb_poseidon2.rs:17-20; mixed heights as vm/src/compiler/recursion/circuit/fri.rs:389-436 verifies them)."""
 
     def __init__(self, ctx: GpuContext, field):
         self.ctx, self.field = ctx, F.field_id(field)
@@ -191,7 +193,8 @@ class MerkleTreeMmcs:
         return root, ProverData(self.ctx, h, root, len(matrices), self.field)
 
     def open_batch(self, index: int, prover_data: ProverData):
-        """(opened rows per matrix, sibling path) at `index` of the tallest matrix."""
+        """(opened rows per matrix, sibling path) at `index` of the tallest matrix
+        (the BatchOpening fri.rs:389-436 checks)."""
         widths = [prover_data.lde_shape(i)[1] for i in range(prover_data.n_mats)]
         rows = np.zeros(sum(widths), dtype=np.uint32)
         path = np.zeros((prover_data.log_max_height, 8), dtype=np.uint32)
@@ -205,7 +208,8 @@ class MerkleTreeMmcs:
 
 
 class Radix2DitParallel:
-    """SC_Dft: coset LDE of a batch of columns."""
+    """SC_Dft: coset LDE of a batch of columns (kb_poseidon2.rs:25; committed row i
+    is x = g * w_N^rev(i), fri.rs:155-171)."""
 
     def __init__(self, ctx: GpuContext, field):
         self.ctx, self.field = ctx, F.field_id(field)
@@ -287,7 +291,8 @@ def last_commit_stats() -> dict:
 
 
 def new_challenger() -> abi.Challenger:
-    """DuplexChallenger::new: zero sponge, empty buffers."""
+    """DuplexChallenger::new: zero sponge, empty buffers (observe / sample as
+    vm/src/compiler/recursion/circuit/challenger.rs:89-106, 223-234)."""
     return abi.Challenger()
 
 
@@ -325,7 +330,8 @@ class TwoAdicFriPcs:
 
     def commit(self, domains_and_traces, plain: bool = False, keep: bool = True):
         """[(domain, trace)] -> (root, ProverData).  LDE shift per matrix is
-        GENERATOR / domain.shift, as TwoAdicFriPcs::commit computes it."""
+        GENERATOR / domain.shift, as TwoAdicFriPcs::commit computes it (called at
+        vm/src/machine/prover.rs:102,244,415,540)."""
         n = len(domains_and_traces)
         mats = (abi.Matrix * n)()
         flags = abi.PICO_COMMIT_PLAIN if plain else 0
@@ -361,7 +367,8 @@ class TwoAdicFriPcs:
 
     def fri_commit_phase(self, codeword, log_final_len: int = 0, betas=None, challenger=None,
                          keep: bool = False) -> FriCommitResult:
-        """FRI commit phase over an EF4 codeword ((2^k, 4) Monty words, bit-reversed order)."""
+        """FRI commit phase over an EF4 codeword ((2^k, 4) Monty words, bit-reversed order;
+        fold and layer commits as fri.rs:288-387 verifies them)."""
         log_n = _log2_exact(codeword.shape[0])
         rounds = log_n - self.log_blowup - log_final_len
         if rounds < 0:
@@ -384,7 +391,9 @@ class TwoAdicFriPcs:
         return FriCommitResult(roots[:rounds], out_betas[:rounds], final, nr.value, data)
 
     def open(self, rounds, challenger, num_queries: int = 84, proof_of_work_bits: int = 16):
-        """TwoAdicFriPcs::open over [(ProverData, points per matrix)]: returns the
+        """TwoAdicFriPcs::open over [(ProverData, points per matrix)] (called at
+        vm/src/machine/prover.rs:589; the proof is what
+        vm/src/compiler/recursion/circuit/fri.rs:77-436 verifies): returns the
         opened values (per batch, matrix, point: (width, 4)) and the proof pieces.
         The challenger is advanced in place, as the prover's is."""
         ob = _OpenBatches(rounds)
