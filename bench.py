@@ -150,6 +150,21 @@ IMAD_PER_SM_CLK = 64
 HASH_TRAFFIC_RATIO = 0.966
 
 
+GOLDEN_ROOTS = ROOT / "tests" / "golden" / "config_roots.json"
+
+
+def root_parity(workload: str, seed: int, roots: dict) -> dict:
+    """The roots the timed steps committed to (device inputs, plain form, host
+    inputs), compared after timing with the root the CPU oracle computed for
+    the same seeded inputs (tests/golden/config_roots.json)."""
+    gold = json.loads(GOLDEN_ROOTS.read_text()).get(workload) if GOLDEN_ROOTS.exists() else None
+    if gold is None or gold["seeds"][0] != seed * 1000:
+        return {"checked": False, "why": "no oracle root for this workload and seed"}
+    ok = {tag: r == gold["root"] for tag, r in roots.items()}
+    return {"checked": True, "root_matches_oracle": all(ok.values()), "per_form": ok,
+            "golden": "tests/golden/config_roots.json (CPU oracle, same seeded inputs)"}
+
+
 def dist_setup(n_gpus: int):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -197,39 +212,48 @@ def job_rate(world: int, cells_per_rank: int, steps: int, max_ms: float) -> floa
 
 
 # ---------------------------------------------------------------- CPU legs
-def cpu_sample_shapes(shapes, field, log_blowup, seconds: float):
-    """A bounded sample of the workload for the CPU: its smallest matrices
-    first, as many as fit in roughly `seconds` of CPU time, calibrated by a
-    short probe."""
-    from oracle import cpu as orc
-    from pico_b200 import fields as F
+# The CPU legs commit a fixed, bounded sample of the workload: its smallest
+# matrices first, up to CPU_SAMPLE_CELLS trace cells (about 10 s on 16 host
+# threads for the uneven KoalaBear shard).  The GPU leg also times a commit of
+# exactly these matrices, so the two rates compare the same work.
+CPU_SAMPLE_CELLS = 1 << 26
 
-    probe = [F.random_matrix(field, 14, 16, 5)]
-    t = time.perf_counter()
-    orc.pcs_commit(field, probe, [F.lde_shift(field)], log_blowup)
-    rate = (16 << 14) / (time.perf_counter() - t)
-    budget = rate * seconds
+
+def cpu_sample(shapes, max_cells: int = CPU_SAMPLE_CELLS):
+    """Indices of the sampled matrices (the workload's own order) and their cells."""
     chosen, tot = [], 0
-    for lh, w in sorted(shapes, key=lambda s: s[1] << s[0]):
-        c = w << lh
-        if tot + c > budget and chosen:
+    for i in sorted(range(len(shapes)), key=lambda i: (shapes[i][1] << shapes[i][0], i)):
+        c = shapes[i][1] << shapes[i][0]
+        if tot + c > max_cells and chosen:
             break
-        chosen.append((lh, w))
+        chosen.append(i)
         tot += c
-    return chosen, tot
+    return sorted(chosen), tot
 
 
-def run_cpu(shapes, field, log_blowup, seed, steps, warmup, seconds):
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_cpu(shapes, field, log_blowup, seed, steps, warmup, max_cells=CPU_SAMPLE_CELLS):
+    """The oracle's TwoAdicFriPcs::commit on the CPU sample (same seeded
+    matrices as the GPU commits), all host threads; median over `steps` runs."""
     from oracle import cpu as orc
     from pico_b200 import fields as F
 
-    sample, cells = cpu_sample_shapes(shapes, field, log_blowup, seconds)
-    mats = [F.random_matrix(field, lh, w, seed * 1000 + i) for i, (lh, w) in enumerate(sample)]
+    idx, cells = cpu_sample(shapes, max_cells)
+    mats = [orc.random_matrix(field, shapes[i][0], shapes[i][1], seed * 1000 + i) for i in idx]
     shifts = [F.lde_shift(field)] * len(mats)
     for _ in range(warmup):
         orc.pcs_commit(field, mats, shifts, log_blowup)
     times = []
-    for _ in range(steps):
+    for _ in range(max(steps, 1)):
         t = time.perf_counter()
         orc.pcs_commit(field, mats, shifts, log_blowup)
         times.append(time.perf_counter() - t)
@@ -238,8 +262,10 @@ def run_cpu(shapes, field, log_blowup, seed, steps, warmup, seconds):
         "value": cells / med,
         "unit": UNIT,
         "cores": orc.num_threads(),
-        "sample": f"{len(sample)} of {len(shapes)} matrices of the workload (smallest first), "
-                  f"{cells} trace cells, median of {steps} runs",
+        "cpu_model": cpu_model(),
+        "sample": f"{len(idx)} of {len(shapes)} matrices of the workload (smallest first, at most "
+                  f"{max_cells} cells): {cells} trace cells, the workload's own seeded inputs; "
+                  f"median of {len(times)} runs",
         "seconds_per_run": med,
     }
 
@@ -274,7 +300,9 @@ def run_gpu(args, rank, world, local):
         root, _ = pcs.commit(list(zip(doms, inputs)), plain=plain, keep=False)
         return root, last_commit_stats()
 
-    def timed(inputs, plain=False):
+    roots = {}
+
+    def timed(inputs, plain=False, tag="device"):
         for _ in range(args.warmup):
             step(inputs, plain)
         barrier(world)
@@ -286,13 +314,15 @@ def run_gpu(args, rank, world, local):
         e0.record()
         stats = []
         for _ in range(args.steps):
-            stats.append(step(inputs, plain)[1])
+            root, st = step(inputs, plain)
+            stats.append(st)
         torch.cuda.synchronize()
         e1.record()
         e1.synchronize()
         clocks = sampler.stop()
         barrier(world)
         ms = allmax(world, e0.elapsed_time(e1))
+        roots[tag] = root.tolist()  # the last timed step's root, checked after timing
         return ms, stats, clocks
 
     ms, stats, clocks = timed(traces)
@@ -300,7 +330,28 @@ def run_gpu(args, rank, world, local):
     value = job_rate(world, cells, args.steps, ms)
 
     # plain per-matrix form (the baseline form), same inputs
-    ms_plain, _, _ = timed(traces, plain=True) if not args.skip_plain else (None, None, None)
+    ms_plain, _, _ = timed(traces, plain=True, tag="plain") if not args.skip_plain else (None, None, None)
+
+    # the CPU legs' sample, committed on the GPU: the same matrices, so the
+    # GPU/CPU ratio compares equal work
+    idx, sample_cells = cpu_sample(shapes, args.cpu_cells)
+    sample_in = [traces[i] for i in idx]
+    sample_pcs_doms = [doms[i] for i in idx]
+
+    def sample_step():
+        pcs.commit(list(zip(sample_pcs_doms, sample_in)), keep=False)
+
+    for _ in range(args.warmup):
+        sample_step()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        sample_step()
+    s1.record()
+    s1.synchronize()
+    sample_ms = s0.elapsed_time(s1) / args.steps
+    del sample_in
 
     # LDE kernels alone (no hashing sharing the SMs): every matrix of the
     # workload through coset_lde_batch, device in and out
@@ -335,7 +386,7 @@ def run_gpu(args, rank, world, local):
         host = [t.cpu().pin_memory().numpy().view(np.uint32) for t in traces]
         del traces
         torch.cuda.empty_cache()
-        ms_e2e, st_e2e, _ = timed(host)
+        ms_e2e, st_e2e, _ = timed(host, tag="host")
         e2e = {
             "value": world * cells * args.steps / (ms_e2e / 1e3),
             "unit": UNIT,
@@ -431,6 +482,10 @@ def run_gpu(args, rank, world, local):
         },
         "phases_ms": {k: float(np.mean([s[k] for s in stats])) for k in ("lde_ms", "leaves_ms", "tree_ms", "total_ms")},
         "e2e": e2e,
+        "parity": root_parity(args.workload, seed, roots),
+        "on_cpu_sample": {"value": sample_cells / (sample_ms / 1e3), "unit": UNIT, "ms_per_step": sample_ms,
+                          "matrices": len(idx), "trace_cells": sample_cells,
+                          "what": "the same commit on the cpu_baseline's sample of matrices (device inputs)"},
     }
     if ms_plain is not None:
         result["plain_form"] = {"value": world * cells * args.steps / (ms_plain / 1e3),
@@ -656,6 +711,11 @@ def run_fri(args):
         e1.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         out[name] = {"ms": ms, "rounds": res.rounds, "elements_per_s": (1 << (log_trace + b)) / (ms / 1e3)}
+        gold = json.loads(GOLDEN_ROOTS.read_text()).get("fri-kb-2^23") if GOLDEN_ROOTS.exists() else None
+        if gold is not None:  # the last timed step's roots, betas and final values against the oracle's
+            g = gold[name]
+            out[name]["matches_oracle"] = (res.roots.tolist() == g["roots"] and res.betas.tolist() == g["betas"]
+                                           and res.final.tolist() == g["final"])
     ctx.close()
     return {
         "metric": "FRI commit-phase codeword elements/sec (EF4, arity 2, Poseidon2 layer commits)",
@@ -832,7 +892,10 @@ def main():
                     help="serving: offered load vs the plain form's one-at-a-time capacity")
     ap.add_argument("--slots", type=int, default=2, help="serving: requests on the device at once")
     ap.add_argument("--mix", choices=list(SERVING_MIXES), default="prover", help="serving: request mix")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="opening workloads: CPU sample size in seconds")
+    ap.add_argument("--cpu-runs", type=int, default=5, help="runs of the CPU baseline (median)")
+    ap.add_argument("--cpu-cells", type=int, default=CPU_SAMPLE_CELLS,
+                    help="commit workloads: trace cells of the CPU sample (smallest matrices first)")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -879,7 +942,7 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             ref = run_cpu(wl["shapes"](), wl["field"], wl["log_blowup"], wl["seed"], args.steps, args.warmup,
-                          args.cpu_seconds)
+                          args.cpu_cells)
             line = {
                 "metric": METRIC, "value": ref["value"], "unit": UNIT, "impl": "reference", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref["seconds_per_run"] * 1e3,
@@ -887,7 +950,7 @@ def main():
                 "data": "synthetic: seeded uniform field elements",
                 "config": {"workload": args.workload, "sample": ref["sample"]},
                 "cpu_baseline": {"value": ref["value"], "unit": UNIT, "cores": ref["cores"], "kind": "port",
-                                 "sample": ref["sample"]},
+                                 "cpu_model": ref["cpu_model"], "sample": ref["sample"]},
                 "e2e": {"value": ref["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "the reference's Rust/Plonky3 CPU path cannot be built here (no cargo, Plonky3 not "
                         "vendored); this is the C + OpenMP restatement (oracle) on all host threads",
@@ -898,9 +961,9 @@ def main():
     result, shapes, field, b = run_gpu(args, rank, world, local)
     if rank == 0:
         if not args.skip_cpu:
-            cpu = run_cpu(shapes, field, b, WORKLOADS[args.workload]["seed"], 1, 0, args.cpu_seconds)
+            cpu = run_cpu(shapes, field, b, WORKLOADS[args.workload]["seed"], args.cpu_runs, 1, args.cpu_cells)
             result["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
-                                      "sample": cpu["sample"]}
+                                      "cpu_model": cpu["cpu_model"], "sample": cpu["sample"]}
         print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist

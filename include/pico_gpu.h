@@ -133,6 +133,14 @@ const char *pico_gpu_last_error(void);
 uint32_t pico_gpu_abi_version(void);
 /* Bytes currently reserved by resident commits / in-flight requests, and the budget. */
 pico_status pico_gpu_memory(pico_ctx *ctx, uint64_t *reserved, uint64_t *budget);
+/* Device bytes a commit of these matrices would reserve against the budget
+ * (pico_gpu_commit / pico_gpu_submit_commit with the same arguments):
+ * `resident` stays reserved until the commit is released (LDEs, digest
+ * layers), `scratch` only while it runs.  Validates the descriptors exactly as
+ * those calls do; needs no device.  No counterpart in the reference (its CPU
+ * commit has no admission step); a serving front end sizes requests with it. */
+pico_status pico_gpu_commit_bytes(pico_field field, const pico_matrix *mats, uint32_t n_mats, uint32_t log_blowup,
+                                  uint32_t flags, uint64_t *resident, uint64_t *scratch);
 
 /* ---- Pcs::commit ---------------------------------------------------------
  * TwoAdicFriPcs::commit (Plonky3 @ brevis-network/Plonky3 f5056c9, called at
@@ -199,6 +207,13 @@ pico_status pico_gpu_coset_lde_batch(pico_ctx *ctx, pico_field field, const uint
  * before any stream capture. */
 pico_status pico_gpu_coset_lde_batch_noalloc(pico_field field, const uint32_t *in, uint32_t log_n, uint32_t width,
                                              uint32_t log_blowup, uint32_t shift, uint32_t *out, void *stream);
+/* Completion check of pico_gpu_coset_lde_batch_noalloc calls: waits for
+ * `stream`, then reports whether any LDE kernel skipped an out-of-range access
+ * since the last check (PICO_ERR_CUDA with the first such access in
+ * pico_gpu_last_error; the result of that call is then wrong) and clears the
+ * record.  Allocates nothing.  The record is per device and shared with the
+ * context-based LDE and commit calls, which report and clear it themselves. */
+pico_status pico_gpu_noalloc_status(void *stream);
 /* MerkleTreeMmcs::commit (SC_ValMmcs, kb_poseidon2.rs:19-20) over matrices
  * that are already extended: mats[i].log_height is the matrix's own height,
  * shift is ignored. */
@@ -331,6 +346,14 @@ pico_status pico_gpu_autotune(pico_ctx *ctx, pico_field field, uint32_t log_n_mi
  * *log_n1_out = log2 n1, or 0 for the one-pass form. */
 pico_status pico_gpu_lde_split(pico_ctx *ctx, pico_field field, uint32_t log_n, uint32_t set_log_n1,
                                uint32_t *log_n1_out);
+
+/* ---- test hook (no counterpart in the reference) ----------------------------
+ * Failure injection on the host: after `after` more device allocations made by
+ * this library (any context, any thread), the next one fails as if the device
+ * were out of memory (PICO_ERR_OUT_OF_MEMORY), then injection switches off;
+ * after < 0 switches it off.  Tests use it to check that a failed commit
+ * returns its budget and buffers and leaves the context usable. */
+pico_status pico_gpu_test_fail_allocations(int64_t after);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,7 @@ def load():
                 ("orc_generator", u32, [C.c_int]),
                 ("orc_num_threads", C.c_int, []),
                 ("orc_set_threads", None, [C.c_int]),
+                ("orc_uniform_monty", None, [C.c_int, u64, u64, vp]),
                 ("orc_permute", C.c_int, [C.c_int, vp, C.c_size_t]),
                 ("orc_permute_canonical", C.c_int, [C.c_int, vp]),
                 ("orc_hash", C.c_int, [C.c_int, vp, C.c_size_t, vp]),
@@ -110,6 +111,16 @@ def set_threads(n: int):
 
 def num_threads() -> int:
     return load().orc_num_threads()
+
+
+def random_matrix(field: int, log_height: int, width: int, seed: int) -> np.ndarray:
+    """The seeded synthetic matrix of pico_b200.fields.random_matrix (the same
+    SplitMix64 stream, Monty form), generated in C for matrices too large for
+    the vectorised numpy form."""
+    out = np.empty((1 << log_height, width), dtype=np.uint32)
+    if out.size:
+        load().orc_uniform_monty(field, seed & 0xFFFFFFFFFFFFFFFF, out.size, out.ctypes.data)
+    return out
 
 
 def permute_canonical(field: int, state) -> np.ndarray:

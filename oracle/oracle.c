@@ -213,6 +213,24 @@ static conv_t conv(const field_t *F) {
 static inline uint32_t c_from(conv_t c, uint32_t x) { return fmul(c.p, x % c.p, c.rinv); }
 static inline uint32_t c_to(conv_t c, uint32_t x) { return fmul(c.p, x, c.r); }
 
+/* Synthetic inputs: SplitMix64 draws >> 33, values >= p skipped (the
+ * generator of pico_b200/fields.py uniform()), converted to Monty form. */
+void orc_uniform_monty(int field, uint64_t seed, uint64_t n, uint32_t *out) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    uint64_t z0 = seed;
+    uint64_t i = 0;
+    while (i < n) {
+        z0 += 0x9E3779B97F4A7C15ull;
+        uint64_t z = z0;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        uint32_t v = (uint32_t)(z >> 33);
+        if (v < F->p) out[i++] = c_to(c, v);
+    }
+}
+
 int orc_permute(int field, uint32_t *states, size_t n) {
     const field_t *F = fld(field);
     conv_t c = conv(F);

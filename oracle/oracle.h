@@ -50,6 +50,11 @@ uint32_t orc_two_adic_generator(int field, uint32_t bits);
 uint32_t orc_generator(int field);
 int orc_num_threads(void);
 void orc_set_threads(int n);
+/* The synthetic-input stream of the benchmarks, in Monty form: output i is the
+ * i-th SplitMix64 draw (state seed + k * 0x9E3779B97F4A7C15, k = 1, 2, ...)
+ * shifted right by 33 whose value is below p; draws >= p are skipped.  The
+ * same stream as pico_b200.fields.uniform, for inputs too large for numpy. */
+void orc_uniform_monty(int field, uint64_t seed, uint64_t n, uint32_t *out);
 
 /* In-place Poseidon2-16 on n states (Monty form). */
 int orc_permute(int field, uint32_t *states, size_t n);

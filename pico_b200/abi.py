@@ -14,7 +14,12 @@ from . import build as _build
 
 PICO_OK = 0
 PICO_ERR_INVALID_ARG = 1
+PICO_ERR_OUT_OF_MEMORY = 2
+PICO_ERR_CUDA = 3
 PICO_ERR_UNSUPPORTED = 4
+PICO_ERR_TIMEOUT = 5
+PICO_ERR_NOT_READY = 6
+PICO_ERR_CANCELLED = 7
 STATUS_NAMES = {
     0: "PICO_OK",
     1: "PICO_ERR_INVALID_ARG",
@@ -138,6 +143,8 @@ SIGNATURES = {
     "pico_gpu_last_error": (C.c_char_p, []),
     "pico_gpu_abi_version": (_u32, []),
     "pico_gpu_memory": (C.c_int, [_vp, C.POINTER(_u64), C.POINTER(_u64)]),
+    "pico_gpu_commit_bytes": (C.c_int, [C.c_int, C.POINTER(Matrix), _u32, _u32, _u32, C.POINTER(_u64),
+                                        C.POINTER(_u64)]),
     "pico_gpu_commit": (C.c_int, [_vp, C.c_int, C.POINTER(Matrix), _u32, _u32, _u32, C.POINTER(_vp), _u32p]),
     "pico_gpu_release": (C.c_int, [_vp, _vp]),
     "pico_gpu_commit_stats": (C.c_int, [_vp, C.POINTER(CommitStats)]),
@@ -149,6 +156,7 @@ SIGNATURES = {
     "pico_gpu_open_batch": (C.c_int, [_vp, _vp, _u64, _vp, _vp]),
     "pico_gpu_coset_lde_batch": (C.c_int, [_vp, C.c_int, _vp, _u32, _u32, _u32, _u32, _vp, _u32]),
     "pico_gpu_coset_lde_batch_noalloc": (C.c_int, [C.c_int, _vp, _u32, _u32, _u32, _u32, _vp, _vp]),
+    "pico_gpu_noalloc_status": (C.c_int, [_vp]),
     "pico_gpu_mmcs_commit": (C.c_int, [_vp, C.c_int, C.POINTER(Matrix), _u32, _u32, C.POINTER(_vp), _u32p]),
     "pico_gpu_poseidon2_permute": (C.c_int, [_vp, C.c_int, _vp, _u64, _u32]),
     "pico_gpu_fri_commit_phase": (
@@ -175,6 +183,7 @@ SIGNATURES = {
     ),
     "pico_gpu_open_values": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp]),
     "pico_gpu_reduced_opening": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp, _vp, _u32, _vp]),
+    "pico_gpu_test_fail_allocations": (C.c_int, [C.c_int64]),
     "pico_gpu_challenger_observe": (C.c_int, [C.c_int, C.POINTER(Challenger), _vp, _u64]),
     "pico_gpu_challenger_sample": (C.c_int, [C.c_int, C.POINTER(Challenger), _vp, _u64]),
 }

@@ -4,6 +4,7 @@
 #include <immintrin.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -317,10 +318,23 @@ uint32_t host_sample(int field, pico_challenger* ch) {
 
 pico_ctx::~pico_ctx() = default;
 
+// Host-side failure injection for tests (pico_gpu_test_fail_allocations):
+// the number of device allocations left before one fails; negative = off.
+static std::atomic<int64_t> g_fail_alloc_after{-1};
+
 static pico_status alloc_async(void** p, size_t bytes, cudaStream_t st) {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
+  if (g_fail_alloc_after.load(std::memory_order_relaxed) >= 0 && g_fail_alloc_after.fetch_sub(1) == 0) {
+    set_error("device allocation: injected failure (pico_gpu_test_fail_allocations)");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
   return cuda_status(cudaMallocAsync(p, bytes, st), "device allocation");
+}
+
+extern "C" pico_status pico_gpu_test_fail_allocations(int64_t after) {
+  g_fail_alloc_after.store(after < 0 ? -1 : after);
+  return PICO_OK;
 }
 
 static void free_async(void* p, cudaStream_t st) {
@@ -468,6 +482,17 @@ extern "C" pico_status pico_gpu_shutdown(pico_ctx* ctx) {
   return PICO_OK;
 }
 
+extern "C" pico_status pico_gpu_commit_bytes(pico_field field, const pico_matrix* mats, uint32_t n_mats,
+                                             uint32_t log_blowup, uint32_t flags, uint64_t* resident,
+                                             uint64_t* scratch) {
+  CommitPlan plan;
+  pico_status s = plan_commit(field, mats, n_mats, log_blowup, flags, true, plan);
+  if (s) return s;
+  if (resident) *resident = plan.bytes_resident;
+  if (scratch) *scratch = plan.bytes_scratch;
+  return PICO_OK;
+}
+
 extern "C" pico_status pico_gpu_memory(pico_ctx* ctx, uint64_t* reserved, uint64_t* budget) {
   if (!ctx) {
     set_error("null context");
@@ -553,6 +578,10 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
     return PICO_ERR_INVALID_ARG;
   }
   const uint32_t S = field_two_adicity(field);
+  if (extend && log_b > kLdeMaxLogBlowup) {
+    set_error("commit: log_blowup %u is above the supported %u", log_b, kLdeMaxLogBlowup);
+    return PICO_ERR_INVALID_ARG;
+  }
   plan = CommitPlan{};
   plan.field = field;
   plan.log_b = extend ? log_b : 0;

@@ -26,8 +26,9 @@ def extract(mod_rs: str):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/vm/src/primitives/mod.rs"
-    nums = extract(src)
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python gen_rc_table.py <path to the pico source tree's vm/src/primitives/mod.rs>")
+    nums = extract(sys.argv[1])
     out = Path(__file__).with_name("p2_rc_table.inc")
     lines = ["/* Poseidon2-16 raw round constants RC_16_30_U32 (30 rounds x 16 lanes),",
              " * extracted by gen_rc_table.py from the reference's",

@@ -154,6 +154,9 @@ struct LdeBatch {
   LdeMat m[kLdeBatch];
 };
 constexpr uint32_t kPwWords = 8192;  // words per (matrix, coset) power table
+// Largest log_blowup an LDE accepts: the coset power tables of one matrix
+// (kPwWords << log_blowup words) are indexed with 32-bit arithmetic.
+constexpr uint32_t kLdeMaxLogBlowup = 16;
 
 // Power tables then LDE kernels for `n` matrices (host descriptors, any
 // count; launched in batches of kLdeBatch).  *launches counts kernels.

@@ -105,6 +105,10 @@ extern "C" pico_status pico_gpu_coset_lde_batch_noalloc(pico_field field, const 
     return PICO_ERR_INVALID_ARG;
   }
   const uint32_t S = field == PICO_KOALABEAR ? 24u : 27u;
+  if (log_blowup > kLdeMaxLogBlowup) {
+    set_error("coset_lde_batch_noalloc: log_blowup %u is above the supported %u", log_blowup, kLdeMaxLogBlowup);
+    return PICO_ERR_INVALID_ARG;
+  }
   if (log_n + log_blowup > S) {
     set_error("coset_lde_batch_noalloc: 2^%u rows with blowup 2^%u exceeds the two-adicity %u", log_n, log_blowup,
               S);
@@ -155,4 +159,24 @@ extern "C" pico_status pico_gpu_coset_lde_batch_noalloc(pico_field field, const 
   tw.hi = tw.lo + kTwiddleWords;
   tw.stage = tw.lo + 2 * kTwiddleWords;
   return cuda_status(launch_lde(field, &L, 1, tw, st), "coset_lde_batch_noalloc launch");
+}
+
+// Bounds-guard verdict of the allocation-free LDE.  Its kernels record a
+// skipped out-of-range access in the LDE unit's device record instead of
+// making it; the call itself is asynchronous and cannot report that, so the
+// caller asks here after its stream has reached the call.  This reads the
+// record into host memory (nothing is allocated) and clears it.
+extern "C" pico_status pico_gpu_noalloc_status(void* stream) {
+  using namespace pico;
+  pico_status rc = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "noalloc_status: stream");
+  if (rc) return rc;
+  GuardRecord g{};
+  if ((rc = cuda_status(lde_guard_fetch(&g, (cudaStream_t)stream), "noalloc_status: guard read-back"))) return rc;
+  if ((rc = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "noalloc_status: guard read-back"))) return rc;
+  if (!g.count) return PICO_OK;
+  set_error("internal bounds guard: LDE kernel skipped %llu access(es); first: tag %llu, offset %llu of %llu, "
+            "block %llu, thread %llu",
+            g.count, g.tag, g.offset, g.extent, g.block, g.thread);
+  lde_guard_clear();
+  return PICO_ERR_CUDA;
 }

@@ -46,6 +46,10 @@ pico_status check_batches(pico_ctx* ctx, const pico_open_batch* b, uint32_t n, u
     set_error("open: no batches");
     return PICO_ERR_INVALID_ARG;
   }
+  if (log_blowup > kLdeMaxLogBlowup) {
+    set_error("open: log_blowup %u is above the supported %u", log_blowup, kLdeMaxLogBlowup);
+    return PICO_ERR_INVALID_ARG;
+  }
   sh = Shape{};
   for (uint32_t i = 0; i < n; i++) {
     const pico_commit* c = b[i].commit;

@@ -328,10 +328,16 @@ class TwoAdicFriPcs:
     def natural_domain_for_degree(self, n: int) -> TwoAdicDomain:
         return TwoAdicDomain(_log2_exact(n), 1)
 
-    def commit(self, domains_and_traces, plain: bool = False, keep: bool = True):
-        """[(domain, trace)] -> (root, ProverData).  LDE shift per matrix is
-        GENERATOR / domain.shift, as TwoAdicFriPcs::commit computes it (called at
-        vm/src/machine/prover.rs:102,244,415,540)."""
+    def commit_bytes(self, domains_and_traces, plain: bool = False):
+        """(resident, scratch) device bytes a commit of these traces reserves
+        against the context's HBM budget (pico_gpu_commit_bytes); no device needed."""
+        mats, flags = self._descriptors(domains_and_traces, plain)
+        res, scr = C.c_uint64(), C.c_uint64()
+        abi.check(abi.load().pico_gpu_commit_bytes(self.field, mats, len(domains_and_traces), self.log_blowup, flags,
+                                                   C.byref(res), C.byref(scr)))
+        return res.value, scr.value
+
+    def _descriptors(self, domains_and_traces, plain: bool):
         n = len(domains_and_traces)
         mats = (abi.Matrix * n)()
         flags = abi.PICO_COMMIT_PLAIN if plain else 0
@@ -353,6 +359,14 @@ class TwoAdicFriPcs:
             mats[k].shift = F.lde_shift(self.field, dom.shift)
             # (n, w, 4) extension traces commit as their base flattening (flatten_to_base)
             mats[k].flags = abi.PICO_MATRIX_EXT4 if ext else 0
+        return mats, flags
+
+    def commit(self, domains_and_traces, plain: bool = False, keep: bool = True):
+        """[(domain, trace)] -> (root, ProverData).  LDE shift per matrix is
+        GENERATOR / domain.shift, as TwoAdicFriPcs::commit computes it (called at
+        vm/src/machine/prover.rs:102,244,415,540)."""
+        n = len(domains_and_traces)
+        mats, flags = self._descriptors(domains_and_traces, plain)
         root = np.zeros(8, dtype=np.uint32)
         h = C.c_void_p()
         abi.check(self.ctx.lib.pico_gpu_commit(

@@ -11,7 +11,7 @@
    height commits and FRI commit phases.  They pin the oracle against
    accidental change; the GPU tests compare against the live oracle too.
 
-Usage: python tests/golden/make_golden.py [reference root]
+Usage: python tests/golden/make_golden.py <root of the pico source tree>
 """
 from __future__ import annotations
 
@@ -47,7 +47,9 @@ def digest(a: np.ndarray) -> str:
 
 
 def main():
-    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <root of the pico source tree>")
+    ref = Path(sys.argv[1])
     kat = {
         "source": "gnark/poseidon2/poseidon2_koalabear_test.go:61-80, gnark/poseidon2/poseidon2_babybear_test.go:58-77",
         "koalabear": {

@@ -20,7 +20,7 @@ def run_bench(*args) -> dict:
 
 
 def test_reference_arm_line():
-    d = run_bench("--impl", "reference", "--steps", "1", "--warmup", "3", "--cpu-seconds", "1")
+    d = run_bench("--impl", "reference", "--steps", "1", "--warmup", "3", "--cpu-cells", str(1 << 20))
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
               "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert k in d, k
@@ -31,6 +31,7 @@ def test_reference_arm_line():
     assert d["value"] > 0 and d["unit"] == "cells/s"
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert cb["cpu_model"]
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0

@@ -1,10 +1,10 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle.
 
-Integer field arithmetic: every comparison is bit-exact.  Small and medium
-shapes compare whole outputs with the oracle; the full-size batched shape is
-checked through size-independent properties (LDE column slices against the
-oracle, Merkle openings verified with the oracle's hash and compression,
-batched == per-matrix form).
+Integer field arithmetic: every comparison is bit-exact.  The shapes here are
+small and medium (heights up to 2^17 for whole-LDE comparisons, 2^19 inside
+commits); every LDE, digest layer and root is compared in full with the
+oracle.  The benchmarked sizes (full-size roots, FRI at 2^23, LDEs of 2^18 ..
+2^22 rows at every split) are in test_gpu_configs.py.
 """
 import numpy as np
 import pytest

@@ -6,7 +6,8 @@ afford cudaMalloc/cudaFree's device-wide synchronisation.  This entry point
 takes its scratch from a fixed array inside the library.  The test calls it
 through the C ABI twice in a row (the second call finds the first call's data
 in the shared scratch) and compares each result bit-exactly with the
-allocating entry point, pico_gpu_coset_lde_batch.  This file sorts last so a
+allocating entry point, pico_gpu_coset_lde_batch, after checking with
+pico_gpu_noalloc_status that no kernel skipped an access.  This file sorts last so a
 run that stops at the first failure has already run every other test.
 """
 import numpy as np
@@ -36,7 +37,8 @@ def test_noalloc_lde_matches_allocating_entry_point(gpu):
             dout = torch.full(((1 << (log_n + b)), w), -1, dtype=torch.int32, device="cuda")
             abi.check(lib.pico_gpu_coset_lde_batch_noalloc(f, din.data_ptr(), log_n, w, b, shift, dout.data_ptr(),
                                                            stream.cuda_stream))
-            stream.synchronize()
+            # waits for the stream and reports any skipped out-of-range access
+            abi.check(lib.pico_gpu_noalloc_status(stream.cuda_stream))
             assert (dout.cpu().numpy().view(np.uint32) == want).all()
 
 
