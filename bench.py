@@ -715,7 +715,7 @@ def run_fri(args):
         if gold is not None:  # the last timed step's roots, betas and final values against the oracle's
             g = gold[name]
             out[name]["matches_oracle"] = (res.roots.tolist() == g["roots"] and res.betas.tolist() == g["betas"]
-                                           and res.final.tolist() == g["final"])
+                                           and res.final_poly.tolist() == g["final"])
     ctx.close()
     return {
         "metric": "FRI commit-phase codeword elements/sec (EF4, arity 2, Poseidon2 layer commits)",

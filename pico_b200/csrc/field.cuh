@@ -135,8 +135,8 @@ struct Ef {
     for (int i = 0; i < 4; i++) r.c[i] = B::mul(a.c[i], s);
     return r;
   }
-  // (a0 + a1 X + a2 X^2 + a3 X^3)(b0 + ...) mod X^4 - W.  Products are
-  // accumulated as 64-bit sums of < p^2 terms and reduced once.
+  // (a0 + a1 X + a2 X^2 + a3 X^3)(b0 + ...) mod X^4 - W: schoolbook, every
+  // product reduced (Montgomery) and summed with modular additions.
   static PICO_HD Ext4 mul(const Ext4& a, const Ext4& b) {
     constexpr uint32_t Wm = (uint32_t)((((uint64_t)F::W) << 32) % F::P);  // Monty(W)
     // high part: X^4.. terms multiplied by W
