@@ -312,6 +312,73 @@ pico_status pico_gpu_reduced_opening(pico_ctx *ctx, const pico_open_batch *batch
                                      uint32_t log_blowup, const uint32_t *values, const uint32_t alpha[4],
                                      uint32_t log_height, uint32_t *out);
 
+/* ---- quotient values (compute_quotient_values, vm/src/machine/utils.rs:201-350,
+ * called from vm/src/machine/prover.rs:457-511) ---------------------------------
+ * A chip's quotient over its quotient domain GENERATOR * <w_Q>,
+ * Q = 2^(log_trace_height + log_quotient_degree), in natural order: for each
+ * point x the chip's constraints are folded as the prover's
+ * ProverConstraintFolder folds them (every assertion: acc = acc * alpha + c,
+ * vm/src/machine/folder.rs:223-227,321-327) over the local row and the next
+ * row (x * w_n), and the value is acc / Z_H(x), with the Lagrange selectors
+ * of vm/src/compiler/recursion/circuit/domain.rs:48-66.
+ *
+ * The traces are read from resident commits (no copy): main is required,
+ * preprocessed and permutation are optional (commit NULL); each must have
+ * been committed with the standard LDE shift and at least Q rows.  The
+ * permutation trace is its base flattening (4 words per extension column,
+ * as PICO_MATRIX_EXT4 commits it).
+ *
+ * The constraints are a straight-line program over 64 base and 16 extension
+ * registers, what a Rust shim emits from the chip's symbolic constraints
+ * (Plonky3 SymbolicExpression): op, dst, a, b per instruction.  For the loads
+ * b = 1 reads the next row.  Constants are Monty form.  public_values (n_public
+ * words), perm_challenges (n_challenges x 4), regional_sum (4, nullable),
+ * global_sum (14 coordinates of the septic digest, nullable), alpha (4).
+ * out: Q x 4 words, host memory unless PICO_OUTPUT_DEVICE.  No counterpart in
+ * the reference's types for the program itself: the reference evaluates the
+ * Rust `eval` directly. */
+typedef enum {
+  PICO_Q_MAIN = 1,        /* base[dst] = main column a (b: next row) */
+  PICO_Q_PREP = 2,        /* base[dst] = preprocessed column a */
+  PICO_Q_PERM = 3,        /* ext[dst] = permutation extension column a */
+  PICO_Q_CONST = 4,       /* base[dst] = a (Monty form) */
+  PICO_Q_PUBLIC = 5,      /* base[dst] = public_values[a] */
+  PICO_Q_FIRST = 6,       /* base[dst] = is_first_row */
+  PICO_Q_LAST = 7,        /* base[dst] = is_last_row */
+  PICO_Q_TRANSITION = 8,  /* base[dst] = is_transition */
+  PICO_Q_ADD = 9,         /* base[dst] = base[a] + base[b]; SUB, MUL alike */
+  PICO_Q_SUB = 10,
+  PICO_Q_MUL = 11,
+  PICO_Q_EADD = 12,       /* ext[dst] = ext[a] + ext[b]; ESUB, EMUL alike */
+  PICO_Q_ESUB = 13,
+  PICO_Q_EMUL = 14,
+  PICO_Q_EMB = 15,        /* ext[dst] = base[a] */
+  PICO_Q_EMULB = 16,      /* ext[dst] = ext[a] * base[b] */
+  PICO_Q_CHALLENGE = 17,  /* ext[dst] = perm_challenges[a] */
+  PICO_Q_REGIONAL = 18,   /* ext[dst] = regional cumulative sum */
+  PICO_Q_GLOBAL = 19,     /* base[dst] = global cumulative sum coordinate a */
+  PICO_Q_ASSERT = 20,     /* acc = acc * alpha + base[a] */
+  PICO_Q_EASSERT = 21     /* acc = acc * alpha + ext[a] */
+} pico_constraint_opcode;
+
+typedef struct {
+  uint32_t op, dst, a, b;
+} pico_constraint_op;
+
+typedef struct {
+  const pico_commit *commit; /* NULL: the trace is absent */
+  uint32_t mat_idx;          /* matrix of the commit (input order) */
+  uint32_t reserved;
+} pico_trace_ref;
+
+pico_status pico_gpu_quotient_values(pico_ctx *ctx, pico_trace_ref preprocessed, pico_trace_ref main,
+                                     pico_trace_ref permutation, uint32_t log_trace_height,
+                                     uint32_t log_quotient_degree, const pico_constraint_op *program,
+                                     uint32_t n_ops, const uint32_t *public_values, uint32_t n_public,
+                                     const uint32_t *perm_challenges, uint32_t n_challenges,
+                                     const uint32_t regional_sum[4], const uint32_t global_sum[14],
+                                     const uint32_t alpha[4], uint32_t *out, uint32_t flags);
+
 /* ---- serving: asynchronous commits ----------------------------------------
  * pico_gpu_submit_commit copies the host matrices it is given before it
  * returns (the caller may reuse them) and queues the commit.  A request is

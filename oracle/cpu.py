@@ -85,6 +85,8 @@ def load():
                 ("orc_pcs_open", C.c_int,
                  [C.c_int, C.POINTER(OpenBatch), u32, u32, u32, u32, C.POINTER(Challenger), vp, vp, vp, vp, vp,
                   vp, vp, vp]),
+                ("orc_quotient_values", C.c_int,
+                 [C.c_int, u32, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp, vp]),
                 ("orc_verify_open", C.c_int,
                  [C.c_int, C.POINTER(OpenBatch), u32, u32, u32, u32, C.POINTER(Challenger), vp, vp, u32, vp, u32,
                   vp, vp]),
@@ -345,3 +347,42 @@ def verify_open(field: int, batches, log_blowup: int, num_queries: int, pow_bits
                                 v.ctypes.data, roots.ctypes.data, len(proof["roots"]), fin.ctypes.data,
                                 int(proof["pow_witness"]), q.ctypes.data, idx.ctypes.data)
     return rc, idx[:num_queries]
+
+
+def quotient_values(field: int, log_trace: int, log_qd: int, program, main_q, prep_q=None, perm_q=None,
+                    public_values=(), perm_challenges=None, regional_sum=None, global_sum=None, alpha=None):
+    """compute_quotient_values (vm/src/machine/utils.rs:201-350) from the traces'
+    evaluations on the quotient domain in natural order (Monty form): main_q and
+    prep_q are (Q, w) base matrices, perm_q is (Q, w, 4) (extension columns).
+    Returns (Q, 4) Monty words."""
+    Q = 1 << (log_trace + log_qd)
+    ops = _u32(program).reshape(-1, 4)
+    m = _u32(main_q)
+    pr = _u32(prep_q) if prep_q is not None else None
+    pe = _u32(perm_q) if perm_q is not None else None
+    pub = _u32(np.asarray(public_values, dtype=np.uint32).reshape(-1))
+    ch = _u32(np.zeros((0, 4), np.uint32) if perm_challenges is None else perm_challenges).reshape(-1, 4)
+    reg = _u32(np.zeros(4, np.uint32) if regional_sum is None else regional_sum)
+    glob = _u32(np.zeros(14, np.uint32) if global_sum is None else global_sum)
+    al = _u32(alpha)
+    out = np.zeros((Q, 4), dtype=np.uint32)
+    _check(load().orc_quotient_values(
+        field, log_trace, log_qd, pr.ctypes.data if pr is not None else None, pr.shape[1] if pr is not None else 0,
+        m.ctypes.data, m.shape[1], pe.ctypes.data if pe is not None else None, pe.shape[1] if pe is not None else 0,
+        ops.ctypes.data, ops.shape[0], pub.ctypes.data if pub.size else None, pub.size,
+        ch.ctypes.data if ch.size else None, ch.shape[0], reg.ctypes.data, glob.ctypes.data, al.ctypes.data,
+        out.ctypes.data), "quotient_values")
+    return out
+
+
+def on_quotient_domain(field: int, trace, log_qd: int):
+    """A trace's evaluations on the quotient domain GENERATOR * <w_Q> in natural
+    order: its coset LDE with blowup 2^log_qd and shift GENERATOR, not
+    bit-reversed (what get_evaluations_on_domain returns, prover.rs:469-489)."""
+    from pico_b200 import fields as F
+
+    t = _u32(trace)
+    if t.ndim == 3:  # extension columns: flatten, extend, restore
+        h, w, _ = t.shape
+        return coset_lde(field, t.reshape(h, 4 * w), log_qd, F.lde_shift(field), bitrev=False).reshape(-1, w, 4)
+    return coset_lde(field, t, log_qd, F.lde_shift(field), bitrev=False)

@@ -1252,3 +1252,116 @@ int orc_verify_open(int field, const orc_open_batch *batches, uint32_t n_batches
     }
     return ORC_OK;
 }
+
+/* ---------------- compute_quotient_values ---------------- */
+/* The prover's quotient computation (vm/src/machine/utils.rs:201-350): per
+ * point x = GENERATOR * w_Q^i of the quotient domain, the chip's constraints
+ * are folded into acc (acc = acc * alpha + c for every assertion, in program
+ * order: ProverConstraintFolder::assert_zero / assert_zero_ext,
+ * vm/src/machine/folder.rs:223-227,321-327) over the local row i and the next
+ * row i + 2^log_qd (cyclically), and the quotient is acc * inv_zerofier.
+ * Selectors for the trace domain H = <w_n> (shift 1), from the verifier's
+ * restatement vm/src/compiler/recursion/circuit/domain.rs:48-66:
+ *   Z_H(x) = x^n - 1, is_first_row = Z_H(x) / (x - 1),
+ *   is_last_row = Z_H(x) / (x - w_n^-1), is_transition = x - w_n^-1,
+ *   inv_zerofier = 1 / Z_H(x).
+ * Canonical arithmetic with Fermat inverses: no batching tricks. */
+#define ORC_QB 64
+#define ORC_QE 16
+int orc_quotient_values(int field, uint32_t log_trace, uint32_t log_qd, const uint32_t *prep, uint32_t prep_w,
+                        const uint32_t *main, uint32_t main_w, const uint32_t *perm, uint32_t perm_w,
+                        const uint32_t *ops, uint32_t n_ops, const uint32_t *pub, uint32_t n_pub,
+                        const uint32_t *chal, uint32_t n_chal, const uint32_t regional[4],
+                        const uint32_t global[14], const uint32_t alpha[4], uint32_t *out) {
+    const field_t *F = fld(field);
+    conv_t c = conv(F);
+    const uint32_t p = F->p, W = F->w_ext;
+    const uint32_t log_q = log_trace + log_qd;
+    if (log_q > F->two_adicity || !main || !ops || !alpha || !out) return ORC_EINVAL;
+    const uint64_t Q = 1ull << log_q, n = 1ull << log_trace;
+    /* validate the program once */
+    for (uint32_t k = 0; k < n_ops; k++) {
+        const uint32_t *o = ops + 4 * k;
+        const uint32_t op = o[0], d = o[1], a = o[2], b = o[3];
+        int ok = 1;
+        switch (op) {
+        case ORC_Q_MAIN: ok = d < ORC_QB && a < main_w && b <= 1; break;
+        case ORC_Q_PREP: ok = d < ORC_QB && prep && a < prep_w && b <= 1; break;
+        case ORC_Q_PERM: ok = d < ORC_QE && perm && a < perm_w && b <= 1; break;
+        case ORC_Q_CONST: ok = d < ORC_QB; break;
+        case ORC_Q_PUBLIC: ok = d < ORC_QB && a < n_pub; break;
+        case ORC_Q_FIRST: case ORC_Q_LAST: case ORC_Q_TRANSITION: ok = d < ORC_QB; break;
+        case ORC_Q_ADD: case ORC_Q_SUB: case ORC_Q_MUL: ok = d < ORC_QB && a < ORC_QB && b < ORC_QB; break;
+        case ORC_Q_EADD: case ORC_Q_ESUB: case ORC_Q_EMUL: ok = d < ORC_QE && a < ORC_QE && b < ORC_QE; break;
+        case ORC_Q_EMB: ok = d < ORC_QE && a < ORC_QB; break;
+        case ORC_Q_EMULB: ok = d < ORC_QE && a < ORC_QE && b < ORC_QB; break;
+        case ORC_Q_CHALLENGE: ok = d < ORC_QE && a < n_chal; break;
+        case ORC_Q_REGIONAL: ok = d < ORC_QE && regional; break;
+        case ORC_Q_GLOBAL: ok = d < ORC_QB && a < 14 && global; break;
+        case ORC_Q_ASSERT: ok = a < ORC_QB; break;
+        case ORC_Q_EASSERT: ok = a < ORC_QE; break;
+        default: ok = 0;
+        }
+        if (!ok) return ORC_EINVAL;
+    }
+    const uint32_t wq = orc_two_adic_generator(field, log_q);
+    const uint32_t wn_inv = finv(p, orc_two_adic_generator(field, log_trace));
+    const uint32_t g = F->generator;
+    uint32_t al[4];
+    for (int i = 0; i < 4; i++) al[i] = c_from(c, alpha[i]);
+    int err = 0;
+#pragma omp parallel for schedule(static)
+    for (long long ii = 0; ii < (long long)Q; ii++) {
+        const uint64_t i = (uint64_t)ii, inext = (i + (1ull << log_qd)) & (Q - 1);
+        const uint32_t x = fmul(p, g, fpow(p, wq, i));
+        const uint32_t zh = fsub(p, fpow(p, x, n), 1);
+        const uint32_t sel_first = fmul(p, zh, finv(p, fsub(p, x, 1)));
+        const uint32_t sel_last = fmul(p, zh, finv(p, fsub(p, x, wn_inv)));
+        const uint32_t sel_trans = fsub(p, x, wn_inv);
+        const uint32_t inv_zh = finv(p, zh);
+        uint32_t rb[ORC_QB] = {0}, re[ORC_QE][4] = {{0}}, acc[4] = {0, 0, 0, 0};
+        for (uint32_t k = 0; k < n_ops; k++) {
+            const uint32_t *o = ops + 4 * k;
+            const uint32_t op = o[0], d = o[1], a = o[2], b = o[3];
+            const uint64_t row = b ? inext : i;
+            uint32_t t[4];
+            switch (op) {
+            case ORC_Q_MAIN: rb[d] = c_from(c, main[row * main_w + a]); break;
+            case ORC_Q_PREP: rb[d] = c_from(c, prep[row * prep_w + a]); break;
+            case ORC_Q_PERM:
+                for (int j = 0; j < 4; j++) re[d][j] = c_from(c, perm[row * 4 * perm_w + 4 * a + j]);
+                break;
+            case ORC_Q_CONST: rb[d] = c_from(c, a); break;
+            case ORC_Q_PUBLIC: rb[d] = c_from(c, pub[a]); break;
+            case ORC_Q_FIRST: rb[d] = sel_first; break;
+            case ORC_Q_LAST: rb[d] = sel_last; break;
+            case ORC_Q_TRANSITION: rb[d] = sel_trans; break;
+            case ORC_Q_ADD: rb[d] = fadd(p, rb[a], rb[b]); break;
+            case ORC_Q_SUB: rb[d] = fsub(p, rb[a], rb[b]); break;
+            case ORC_Q_MUL: rb[d] = fmul(p, rb[a], rb[b]); break;
+            case ORC_Q_EADD: for (int j = 0; j < 4; j++) t[j] = fadd(p, re[a][j], re[b][j]); memcpy(re[d], t, 16); break;
+            case ORC_Q_ESUB: for (int j = 0; j < 4; j++) t[j] = fsub(p, re[a][j], re[b][j]); memcpy(re[d], t, 16); break;
+            case ORC_Q_EMUL: ext_mul_c(p, W, re[a], re[b], t); memcpy(re[d], t, 16); break;
+            case ORC_Q_EMB: re[d][0] = rb[a]; re[d][1] = re[d][2] = re[d][3] = 0; break;
+            case ORC_Q_EMULB: for (int j = 0; j < 4; j++) t[j] = fmul(p, re[a][j], rb[b]); memcpy(re[d], t, 16); break;
+            case ORC_Q_CHALLENGE: for (int j = 0; j < 4; j++) re[d][j] = c_from(c, chal[4 * a + j]); break;
+            case ORC_Q_REGIONAL: for (int j = 0; j < 4; j++) re[d][j] = c_from(c, regional[j]); break;
+            case ORC_Q_GLOBAL: rb[d] = c_from(c, global[a]); break;
+            case ORC_Q_ASSERT:
+                ext_mul_c(p, W, acc, al, t);
+                t[0] = fadd(p, t[0], rb[a]);
+                memcpy(acc, t, 16);
+                break;
+            case ORC_Q_EASSERT:
+                ext_mul_c(p, W, acc, al, t);
+                for (int j = 0; j < 4; j++) acc[j] = fadd(p, t[j], re[a][j]);
+                break;
+            default:
+#pragma omp atomic write
+                err = 1;
+            }
+        }
+        for (int j = 0; j < 4; j++) out[4 * i + j] = c_to(c, fmul(p, acc[j], inv_zh));
+    }
+    return err ? ORC_EINVAL : ORC_OK;
+}

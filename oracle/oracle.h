@@ -166,6 +166,33 @@ int orc_verify_open(int field, const orc_open_batch *batches, uint32_t n_batches
                     const uint32_t *roots, uint32_t n_rounds, const uint32_t final_poly[4], uint32_t pow_witness,
                     const uint32_t *queries, uint32_t *indices_out);
 
+/* ---- compute_quotient_values (vm/src/machine/utils.rs:201-350) ----------
+ * A chip's constraints as a register program (the same op list the GPU entry
+ * point pico_gpu_quotient_values takes): op, dst, a, b per instruction, base
+ * registers (< 64) and extension registers (< 16).  Folded as the prover's
+ * ProverConstraintFolder does (vm/src/machine/folder.rs:223-227,321-327):
+ * each assertion does acc = acc * alpha + x; the quotient at a point is
+ * acc / Z_H(x), with the Lagrange selectors of
+ * vm/src/compiler/recursion/circuit/domain.rs:48-66 (trace domain shift 1).
+ * Inputs are the traces' evaluations on the quotient domain
+ * GENERATOR * <w_Q>, Q = 2^(log_trace + log_qd), in natural order (Monty
+ * form); `prep` or `perm` may be NULL (absent), `perm` rows hold perm_w
+ * extension elements (4 words each).  `global` holds the global cumulative
+ * sum's 14 coordinates.  out: Q x 4 words (Monty). */
+enum {
+    ORC_Q_MAIN = 1, ORC_Q_PREP = 2, ORC_Q_PERM = 3, ORC_Q_CONST = 4, ORC_Q_PUBLIC = 5,
+    ORC_Q_FIRST = 6, ORC_Q_LAST = 7, ORC_Q_TRANSITION = 8,
+    ORC_Q_ADD = 9, ORC_Q_SUB = 10, ORC_Q_MUL = 11,
+    ORC_Q_EADD = 12, ORC_Q_ESUB = 13, ORC_Q_EMUL = 14, ORC_Q_EMB = 15, ORC_Q_EMULB = 16,
+    ORC_Q_CHALLENGE = 17, ORC_Q_REGIONAL = 18, ORC_Q_GLOBAL = 19,
+    ORC_Q_ASSERT = 20, ORC_Q_EASSERT = 21
+};
+int orc_quotient_values(int field, uint32_t log_trace, uint32_t log_qd, const uint32_t *prep, uint32_t prep_w,
+                        const uint32_t *main, uint32_t main_w, const uint32_t *perm, uint32_t perm_w,
+                        const uint32_t *ops, uint32_t n_ops, const uint32_t *pub, uint32_t n_pub,
+                        const uint32_t *chal, uint32_t n_chal, const uint32_t regional[4],
+                        const uint32_t global[14], const uint32_t alpha[4], uint32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -131,6 +131,10 @@ class OpenStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TraceRef(C.Structure):
+    _fields_ = [("commit", C.c_void_p), ("mat_idx", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 _u32p = C.POINTER(C.c_uint32)
 _vp = C.c_void_p
 _u32 = C.c_uint32
@@ -184,6 +188,10 @@ SIGNATURES = {
     "pico_gpu_open_values": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp]),
     "pico_gpu_reduced_opening": (C.c_int, [_vp, C.POINTER(OpenBatch), _u32, _u32, _vp, _vp, _u32, _vp]),
     "pico_gpu_test_fail_allocations": (C.c_int, [C.c_int64]),
+    "pico_gpu_quotient_values": (
+        C.c_int,
+        [_vp, TraceRef, TraceRef, TraceRef, _u32, _u32, _vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _u32],
+    ),
     "pico_gpu_challenger_observe": (C.c_int, [C.c_int, C.POINTER(Challenger), _vp, _u64]),
     "pico_gpu_challenger_sample": (C.c_int, [C.c_int, C.POINTER(Challenger), _vp, _u64]),
 }

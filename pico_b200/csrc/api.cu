@@ -9,7 +9,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "field.cuh"
@@ -331,6 +333,10 @@ static pico_status alloc_async(void** p, size_t bytes, cudaStream_t st) {
   }
   return cuda_status(cudaMallocAsync(p, bytes, st), "device allocation");
 }
+
+namespace pico {
+pico_status device_alloc(void** p, size_t bytes, cudaStream_t st) { return alloc_async(p, bytes, st); }
+}  // namespace pico
 
 extern "C" pico_status pico_gpu_test_fail_allocations(int64_t after) {
   g_fail_alloc_after.store(after < 0 ? -1 : after);
@@ -1146,6 +1152,39 @@ pico_commit::~pico_commit() { destroy_events(); }
 
 static thread_local pico_commit_stats g_last_stats{};
 
+namespace pico {
+// Per-commit and per-request metrics: with PICO_METRICS_LOG set to a path,
+// every finished commit (and every served request, with its queue and run
+// times) appends one JSON line to that file.  The reference's counterpart is
+// its per-chunk proving-time table (vm/src/instances/machine/riscv.rs:255-266).
+static std::mutex g_metrics_mu;
+void metrics_record(const char* kind, int field, uint32_t n_mats, uint32_t log_b, uint32_t flags,
+                    const pico_commit_stats& st, double queued_us, double run_us) {
+  const char* path = getenv("PICO_METRICS_LOG");
+  if (!path || !*path) return;
+  const double ts = std::chrono::duration<double>(std::chrono::system_clock::now().time_since_epoch()).count();
+  char line[768];
+  int n = snprintf(line, sizeof line,
+                   "{\"ts\": %.6f, \"kind\": \"%s\", \"field\": \"%s\", \"matrices\": %u, \"log_blowup\": %u, "
+                   "\"input\": \"%s\", \"form\": \"%s\", \"cells\": %llu, \"lde_cells\": %llu, "
+                   "\"permutations\": %llu, \"launches\": %llu, \"total_ms\": %.4f, \"h2d_ms\": %.4f, "
+                   "\"lde_ms\": %.4f, \"leaves_ms\": %.4f, \"tree_ms\": %.4f",
+                   ts, kind, field == 0 ? "koalabear" : "babybear", n_mats, log_b,
+                   (flags & PICO_INPUT_DEVICE) ? "device" : "host", (flags & PICO_COMMIT_PLAIN) ? "plain" : "batched",
+                   (unsigned long long)st.cells, (unsigned long long)st.lde_cells,
+                   (unsigned long long)st.permutations, (unsigned long long)st.launches, st.total_ms, st.h2d_ms,
+                   st.lde_ms, st.leaves_ms, st.tree_ms);
+  if (queued_us >= 0 && n > 0 && n < (int)sizeof line)
+    n += snprintf(line + n, sizeof line - n, ", \"queued_us\": %.1f, \"run_us\": %.1f", queued_us, run_us);
+  if (n <= 0 || n >= (int)sizeof line - 3) return;
+  std::lock_guard<std::mutex> g(g_metrics_mu);
+  if (FILE* f = fopen(path, "a")) {
+    fprintf(f, "%s}\n", line);
+    fclose(f);
+  }
+}
+}  // namespace pico
+
 // ---------------------------------------------------------------------------
 // Synchronous commit
 
@@ -1192,6 +1231,7 @@ static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_mat
   memcpy(root, root_h, 32);
   finish_stats(c.get());
   g_last_stats = c->stats;
+  metrics_record(extend ? "commit" : "mmcs_commit", field, n_mats, extend ? log_blowup : 0, flags, c->stats, -1, -1);
   if (out) {
     *out = c.release();
   } else {
@@ -1486,6 +1526,53 @@ extern "C" pico_status pico_gpu_lde_split(pico_ctx* ctx, pico_field field, uint3
   return PICO_OK;
 }
 
+// Autotuner cache: with PICO_TUNE_CACHE set to a path, pico_gpu_autotune
+// takes the choices recorded there for this device model (name and SM count)
+// instead of timing them again, and appends what it times.  One line per
+// choice: "<device>|<sms> <field> split <log_n> <log_n1>" or
+// "<device>|<sms> <field> hash <block> 0".
+namespace {
+std::mutex g_tune_mu;
+std::string tune_device_key(int device) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return "unknown";
+  std::string name(prop.name);
+  for (char& ch : name)
+    if (ch == ' ') ch = '_';
+  return name + "|" + std::to_string(prop.multiProcessorCount);
+}
+struct TuneCache {
+  std::map<uint32_t, uint32_t> split;  // log_n -> log_n1
+  uint32_t hash_block = 0;
+};
+TuneCache tune_cache_load(const char* path, const std::string& key, int field) {
+  TuneCache c;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  FILE* f = fopen(path, "r");
+  if (!f) return c;
+  char dev[256], kind[16];
+  int fld;
+  unsigned a, b;
+  while (fscanf(f, "%255s %d %15s %u %u", dev, &fld, kind, &a, &b) == 5) {
+    if (key != dev || fld != field) continue;
+    if (!strcmp(kind, "split") && pico::lde_split_valid(a, b)) c.split[a] = b;
+    if (!strcmp(kind, "hash") && (a == 64 || a == 128 || a == 256)) c.hash_block = a;
+  }
+  fclose(f);
+  return c;
+}
+void tune_cache_append(const char* path, const std::string& key, int field, const std::vector<std::pair<uint32_t, uint32_t>>& splits,
+                       uint32_t hash_block) {
+  if (splits.empty() && !hash_block) return;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  for (auto& sp : splits) fprintf(f, "%s %d split %u %u\n", key.c_str(), field, sp.first, sp.second);
+  if (hash_block) fprintf(f, "%s %d hash %u 0\n", key.c_str(), field, hash_block);
+  fclose(f);
+}
+}  // namespace
+
 extern "C" pico_status pico_gpu_autotune(pico_ctx* ctx, pico_field field, uint32_t log_n_min, uint32_t log_n_max,
                                          float* ms_out) {
   using namespace pico;
@@ -1493,6 +1580,12 @@ extern "C" pico_status pico_gpu_autotune(pico_ctx* ctx, pico_field field, uint32
     set_error("autotune: bad arguments");
     return PICO_ERR_INVALID_ARG;
   }
+  const char* cache_path = getenv("PICO_TUNE_CACHE");
+  const bool use_cache = cache_path && *cache_path;
+  const std::string dev_key = use_cache ? tune_device_key(ctx->device) : std::string();
+  const TuneCache cached = use_cache ? tune_cache_load(cache_path, dev_key, field) : TuneCache{};
+  std::vector<std::pair<uint32_t, uint32_t>> timed_splits;
+  uint32_t timed_block = 0;
   const uint32_t lo = std::max<uint32_t>(log_n_min, kLdeSmallMaxLog + 1);
   const uint32_t hi = std::min<uint32_t>(log_n_max, std::min<uint32_t>(kLdeMaxLogN, field_two_adicity(field) - 1));
   cudaSetDevice(ctx->device);
@@ -1546,6 +1639,13 @@ extern "C" pico_status pico_gpu_autotune(pico_ctx* ctx, pico_field field, uint32
       const uint32_t def = (l + 1) / 2;
       float best = 0;
       uint32_t best_n1 = 0;
+      if (auto it = cached.split.find(l); it != cached.split.end()) {
+        // from the cache: not timed; the chosen split's time reads -1
+        ctx->lde_split[field][l] = (uint8_t)it->second;
+        if (ms_out)
+          for (int c = 0; c < 3; c++) ms_out[3 * (l - log_n_min) + c] = (def - 1 + c == it->second) ? -1.0f : 0.0f;
+        continue;
+      }
       for (int c = 0; c < 3; c++) {
         const uint32_t n1 = def - 1 + c;
         float ms = 0;
@@ -1570,7 +1670,16 @@ extern "C" pico_status pico_gpu_autotune(pico_ctx* ctx, pico_field field, uint32
         }
         if (ms_out) ms_out[3 * (l - log_n_min) + c] = ms;
       }
-      if (best_n1) ctx->lde_split[field][l] = (uint8_t)best_n1;
+      if (best_n1) {
+        ctx->lde_split[field][l] = (uint8_t)best_n1;
+        timed_splits.push_back({l, best_n1});
+      }
+    }
+    if (cached.hash_block) {
+      ctx->hash_block[field] = cached.hash_block;
+      if (ms_out)
+        for (int c = 0; c < 3; c++) ms_out[3 * (log_n_max - log_n_min + 1) + c] = (64u << c) == cached.hash_block ? -1.0f : 0.0f;
+      return PICO_OK;
     }
     RowGroup g;
     memset(&g, 0, sizeof g);
@@ -1594,9 +1703,11 @@ extern "C" pico_status pico_gpu_autotune(pico_ctx* ctx, pico_field field, uint32
       if (ms_out) ms_out[3 * (log_n_max - log_n_min + 1) + c] = ms;
     }
     ctx->hash_block[field] = best_block;
+    timed_block = best_block;
     return PICO_OK;
   };
   pico_status s = run();
+  if (!s && use_cache) tune_cache_append(cache_path, dev_key, field, timed_splits, timed_block);
   for (void* p : bufs) cudaFreeAsync(p, st);
   if (!s) s = guard_enqueue(ctx, slot, st);
   pico_status s2 = cuda_status(cudaStreamSynchronize(st), "autotune");

@@ -12,7 +12,7 @@
 //
 // Costs and rules of the static arrays:
 //   - every GPU that loads this library holds kNoAllocScratchWords * 4 bytes
-//     (32 MiB) plus 384 KiB of twiddles until the process exits;
+//     (32 MiB) plus 512 KiB of twiddle tables until the process exits;
 //   - all calls share the one scratch array: calls that overlap on the GPU
 //     (two streams, or two host threads) race on it and corrupt each other's
 //     results; serialise them on one stream;

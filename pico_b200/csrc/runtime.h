@@ -59,6 +59,9 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
 
 struct Server;  // serving.h
 
+// Stream-ordered device allocation of the library (failure injection for
+// tests included); free with cudaFreeAsync on a stream ordered after st.
+pico_status device_alloc(void** p, size_t bytes, cudaStream_t st);
 bool try_reserve(pico_ctx* ctx, uint64_t bytes);
 void unreserve(pico_ctx* ctx, uint64_t bytes);
 cudaStream_t pick_stream(pico_ctx* ctx, cudaStream_t* copy_stream = nullptr, uint32_t* slot = nullptr);
@@ -85,6 +88,10 @@ pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& 
 pico_status guard_enqueue(pico_ctx* ctx, uint32_t slot, cudaStream_t st);
 pico_status guard_verdict(pico_ctx* ctx, uint32_t slot, std::string* msg = nullptr);
 pico_status finish_stats(pico_commit* c);
+// One JSON line per finished commit or served request into the file named by
+// PICO_METRICS_LOG (nothing when unset); queued_us < 0 for synchronous commits.
+void metrics_record(const char* kind, int field, uint32_t n_mats, uint32_t log_b, uint32_t flags,
+                    const pico_commit_stats& st, double queued_us, double run_us);
 
 }  // namespace pico
 

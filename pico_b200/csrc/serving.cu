@@ -16,6 +16,7 @@
 //   - LDEs and digest layers stay resident (and budgeted) until the caller
 //     releases the commit handed over by pico_gpu_wait.
 #include <chrono>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <list>
@@ -287,6 +288,13 @@ extern "C" pico_status pico_gpu_wait(pico_ctx* ctx, pico_request* req, int64_t t
   req->commit = nullptr;
   req->state = pico_request::TAKEN;
   lk.unlock();
+  if (c && getenv("PICO_METRICS_LOG")) {
+    finish_stats(c);
+    const uint32_t fl = (req->plan.input_device ? PICO_INPUT_DEVICE : 0u) | (req->plan.plain ? PICO_COMMIT_PLAIN : 0u);
+    metrics_record("request", req->plan.field, (uint32_t)req->plan.mats.size(), req->plan.log_b, fl, c->stats,
+                   std::chrono::duration<double, std::micro>(req->t_admit - req->t_submit).count(),
+                   std::chrono::duration<double, std::micro>(req->t_done - req->t_admit).count());
+  }
   if (out) {
     *out = c;
   } else if (c) {

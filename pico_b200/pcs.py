@@ -80,10 +80,18 @@ class GpuContext:
         abi.check(self.lib.pico_gpu_autotune(self.handle, f, log_n_min, log_n_max, ms))
         out = {}
         for i, l in enumerate(range(log_n_min, log_n_max + 1)):
+            if any(ms[3 * i + c] < 0 for c in range(3)):  # taken from the PICO_TUNE_CACHE file
+                out[l] = {"log_n1": self.lde_split(f, l), "ms": {}, "cached": True}
+                continue
             times = {(l + 1) // 2 - 1 + c: ms[3 * i + c] for c in range(3) if ms[3 * i + c] > 0}
             if times:
                 out[l] = {"log_n1": self.lde_split(f, l), "ms": times}
-        out["hash_block"] = {64 << c: ms[3 * heights + c] for c in range(3)}
+        hb = [ms[3 * heights + c] for c in range(3)]
+        if any(v < 0 for v in hb):
+            out["hash_block"] = {64 << c: (1.0 if hb[c] < 0 else 2.0) for c in range(3)}  # cached choice ranks first
+            out["hash_block_cached"] = True
+        else:
+            out["hash_block"] = {64 << c: hb[c] for c in range(3)}
         return out
 
     def lde_split(self, field, log_n: int, set_log_n1: int = 0) -> int:

@@ -21,6 +21,7 @@ STRUCTS = {
     "OpenBatch": "pico_open_batch",
     "FriParams": "pico_fri_params",
     "OpenStats": "pico_open_stats",
+    "TraceRef": "pico_trace_ref",
 }
 
 
