@@ -8,7 +8,6 @@
 // observing the root and sampling beta on the device, then the fold.
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -18,40 +17,63 @@
 using namespace pico;
 
 namespace pico {
-// One fused launch per round (k_fri_round: fold of the previous codeword,
-// leaf hashing, the whole tree, the challenger step), then the last fold.
 pico_status enqueue_fri_rounds(int field, cudaStream_t st, const TwiddleTables& tw, uint32_t log_n, uint32_t R,
                                const std::vector<uint32_t*>& codewords, const std::vector<uint32_t*>& trees,
                                uint32_t* d_betas, DevChallenger* d_ch, const uint32_t* const* inject,
                                uint32_t* launches) {
-  if (launches) *launches = 0;
-  if (R == 0) return PICO_OK;
   pico_status s;
-  // promotion counters, zero before each round's launch (the kernel re-zeroes those it uses)
-  const uint32_t nc = std::max<uint32_t>(1u, fri_round_counters(log_n - 1));
-  uint32_t* counters = nullptr;
-  if ((s = device_alloc((void**)&counters, 4ull * nc, st))) return s;
-  s = cuda_status(cudaMemsetAsync(counters, 0, 4ull * nc, st), "FRI counters");
   uint32_t nl = 0;
-  for (uint32_t r = 0; r < R && !s; r++) {
-    const uint32_t L = log_n - r;  // codeword length 2^L: 2^(L-1) leaves
-    const bool fold = r > 0;
-    s = cuda_status(launch_fri_round(field, fold, fold ? codewords[r - 1] : codewords[0],
-                                     fold ? d_betas + 4 * (r - 1) : nullptr,
-                                     fold && inject ? inject[r - 1] : nullptr, fold ? codewords[r] : nullptr,
-                                     trees[r], L - 1, counters, d_ch, d_betas + 4 * r, tw, st),
-                    "FRI round");
+  for (uint32_t r = 0; r < R; r++) {
+    const uint32_t L = log_n - r;            // codeword length 2^L
+    const uint64_t leaves = 1ull << (L - 1);  // rows of the (len/2) x 8 matrix
+    if (r == 0) {
+      // later rounds' leaves come out of the previous round's fold
+      RowGroup g;
+      memset(&g, 0, sizeof g);
+      g.n_segs = 1;
+      g.total_width = 8;
+      g.segs[0].ptr = codewords[0];
+      g.segs[0].width = 8;
+      if ((s = cuda_status(launch_hash_rows(field, g, leaves, trees[0], st), "FRI leaf hashing"))) return s;
+      nl++;
+    }
+    // wide levels one launch each; from 2^15 nodes down, seven levels per
+    // launch (k_subtree_quad); the last <= 512 nodes and the challenger in
+    // one block
+    uint32_t* layer = trees[r];
+    uint64_t n = leaves;
+    while (n > 512) {
+      if (n <= (1u << 15)) {
+        if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)n, SubtreeInj{}, st), "FRI subtree"))) return s;
+        nl++;
+        for (int l = 0; l < 7; l++) {
+          layer += n * 8;
+          n /= 2;
+        }
+        continue;
+      }
+      uint32_t* next = layer + n * 8;
+      if ((s = cuda_status(launch_compress(field, layer, next, n / 2, nullptr, st), "FRI compression"))) return s;
+      nl++;
+      layer = next;
+      n /= 2;
+    }
+    if ((s = cuda_status(launch_tree_top(field, layer, (uint32_t)n, d_ch, d_betas + 4 * r, st), "FRI tree top")))
+      return s;
+    nl++;
+    const uint32_t* inj = inject ? inject[r] : nullptr;
+    if (r + 1 < R)
+      s = cuda_status(launch_fri_fold_hash(field, codewords[r], L, d_betas + 4 * r, tw, codewords[r + 1], inj,
+                                           trees[r + 1], st),
+                      "fold and hash");
+    else
+      s = cuda_status(launch_fri_fold_tw(field, codewords[r], L, d_betas + 4 * r, tw, codewords[r + 1], st, inj),
+                      "fold");
+    if (s) return s;
     nl++;
   }
-  if (!s) {
-    s = cuda_status(launch_fri_fold_tw(field, codewords[R - 1], log_n - R + 1, d_betas + 4 * (R - 1), tw,
-                                       codewords[R], st, inject ? inject[R - 1] : nullptr),
-                    "fold");
-    nl++;
-  }
-  cudaFreeAsync(counters, st);
   if (launches) *launches = nl;
-  return s;
+  return PICO_OK;
 }
 }  // namespace pico
 

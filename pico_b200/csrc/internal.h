@@ -128,17 +128,6 @@ cudaError_t launch_challenger_round(int field, DevChallenger* ch, const uint32_t
                                     cudaStream_t st);
 // Levels above `level` (n_in <= 512 digests, a power of two) up to the root,
 // written after it; with ch, then observe the root and sample beta_out (4 words).
-// One whole FRI commit round (k_fri_round): with `fold`, fold cw_in (the
-// previous codeword, 2^(log_leaves + 2) EF4) with beta_in (+ inject) into
-// cw_out; hash this round's 2^log_leaves leaves (rows pairs of cw_out, or of
-// cw_in without fold) and build its whole tree; with ch, observe the root and
-// sample beta_out.  counters: fri_round_counters(log_leaves) words, zero
-// before the launch and zero again after it.
-uint32_t fri_round_counters(uint32_t log_leaves);
-cudaError_t launch_fri_round(int field, bool fold, const uint32_t* cw_in, const uint32_t* beta_in,
-                             const uint32_t* inject, uint32_t* cw_out, uint32_t* tree, uint32_t log_leaves,
-                             uint32_t* counters, DevChallenger* ch, uint32_t* beta_out, TwiddleTables tw,
-                             cudaStream_t st);
 cudaError_t launch_tree_top(int field, uint32_t* level, uint32_t n_in, DevChallenger* ch, uint32_t* beta_out,
                             cudaStream_t st);
 // Observe n elements at vals.

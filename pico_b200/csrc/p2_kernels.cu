@@ -577,194 +577,6 @@ __global__ void __launch_bounds__(256) k_tree_top(uint32_t* level, uint32_t n_in
   }
 }
 
-// ---------------------------------------------------------------------------
-// One FRI commit round in one launch (rounds of TwoAdicFriPcs::open's commit
-// phase, verified at vm/src/compiler/recursion/circuit/fri.rs:45-52,288-387).
-// CTA c owns leaves [256 c, 256 c + 256): with FOLD it first folds the
-// previous round's codeword rows 2k and 2k+1 into this round's codeword
-// (adding the injected reduced opening), then hashes each pair as one
-// 8-element leaf, then reduces its 256 leaves to one node in shared memory,
-// writing every level into the round's tree.  The CTA that finishes last in
-// a group of 256 (an atomic counter per group, reset by that CTA for the next
-// launch) reduces the group's 256 nodes by eight more levels, and so on up to
-// the root; the CTA that computes the root runs the challenger step (observe
-// the root, sample beta).  Nothing waits: a CTA either finishes or carries on
-// with work whose inputs are complete (each writer fences its nodes before
-// its atomic increment).  Compared with one launch per compression level,
-// the eight levels above each leaf stay in shared memory and there are no
-// launch gaps between levels.
-constexpr uint32_t kFriRoundCta = 256;  // leaves per CTA, and nodes per promotion group
-
-struct FriRoundArgs {
-  const uint32_t* cw_in;   // FOLD: previous codeword (2^(log_leaves + 2) EF4); else this round's
-  const uint32_t* beta_in; // FOLD: previous round's beta (4 words)
-  const uint32_t* inject;  // FOLD: reduced opening added to the folded rows (nullable)
-  uint32_t* cw_out;        // FOLD: this round's codeword (2^(log_leaves + 1) EF4)
-  uint32_t* tree;          // this round's digest layers, leaves first
-  uint32_t* counters;      // zero before the launch; zero again after it
-  DevChallenger* ch;       // nullable: betas are given
-  uint32_t* beta_out;      // this round's beta (with ch)
-  uint32_t log_leaves;
-};
-
-// Digest-layer offset (words) of level l of a tree over 2^log_leaves leaves.
-__device__ __forceinline__ uint64_t layer_words(uint32_t log_leaves, uint32_t l) {
-  return 8ull * ((2ull << log_leaves) - ((2ull << log_leaves) >> l));
-}
-
-// Reduce the n (a power of two, at most 256) nodes in buf, which are nodes
-// [base, base + n) of level lvl, to one; every computed level is written to
-// the tree.  The result is left in buf[0..8).
-template <class F>
-__device__ void cta_reduce(uint32_t* buf, uint32_t n, uint32_t lvl, uint64_t base, uint32_t* tree,
-                           uint32_t log_leaves) {
-  const uint32_t tid = threadIdx.x;
-  while (n > 1) {
-    const uint32_t m = n >> 1;
-    lvl++;
-    base >>= 1;
-    uint32_t* out = tree + layer_words(log_leaves, lvl) + base * 8;
-    if (m > 64) {
-      uint32_t st[16];
-      if (tid < m) {
-#pragma unroll
-        for (int k = 0; k < 16; k++) st[k] = buf[16 * tid + k];
-        p2_permute<F>(st);
-      }
-      __syncthreads();
-      if (tid < m) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          buf[8 * tid + k] = st[k];
-          out[8 * tid + k] = st[k];
-        }
-      }
-    } else {
-      const uint32_t node = tid >> 2, q = tid & 3;
-      uint32_t v[4];
-      if (tid < 4 * m) {
-        const unsigned mask = 4 * m >= 32 ? 0xffffffffu : ((1u << (4 * m)) - 1u);
-#pragma unroll
-        for (int k = 0; k < 4; k++) v[k] = buf[16 * node + 4 * q + k];
-        p2_permute_quad<F>(v, q, mask);
-      }
-      __syncthreads();
-      if (tid < 4 * m && q < 2) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          buf[8 * node + 4 * q + k] = v[k];
-          out[8 * node + 4 * q + k] = v[k];
-        }
-      }
-    }
-    __syncthreads();
-    n = m;
-  }
-}
-
-template <class F, bool FOLD>
-__global__ void __launch_bounds__(kFriRoundCta) k_fri_round(const __grid_constant__ FriRoundArgs A,
-                                                            const __grid_constant__ TwiddleTables tw) {
-  __shared__ uint32_t buf[kFriRoundCta * 8];
-  __shared__ uint32_t s_last;
-  const uint32_t tid = threadIdx.x;
-  const uint64_t n_leaves = 1ull << A.log_leaves;
-  const uint32_t here = n_leaves < kFriRoundCta ? (uint32_t)n_leaves : kFriRoundCta;
-  const uint64_t base = (uint64_t)blockIdx.x * kFriRoundCta;
-  if (tid < here) {
-    const uint64_t k = base + tid;
-    uint32_t s[16];
-    if constexpr (FOLD) {
-      const Ext4 hb = half_beta<F>(A.beta_in);
-#pragma unroll
-      for (int u = 0; u < 2; u++) {
-        const uint64_t r = 2 * k + u;
-        Ext4 res = fri_fold_row<F>(A.cw_in, A.log_leaves + 2, r, hb, tw);
-        if (A.inject) {
-          const uint4 v = __ldg(reinterpret_cast<const uint4*>(A.inject) + r);
-          res = Ef<F>::add(res, Ext4{{v.x, v.y, v.z, v.w}});
-        }
-        reinterpret_cast<uint4*>(A.cw_out)[r] = make_uint4(res.c[0], res.c[1], res.c[2], res.c[3]);
-#pragma unroll
-        for (int i = 0; i < 4; i++) s[4 * u + i] = res.c[i];
-      }
-    } else {
-      const uint4 a = __ldg(reinterpret_cast<const uint4*>(A.cw_in) + 2 * k);
-      const uint4 b = __ldg(reinterpret_cast<const uint4*>(A.cw_in) + 2 * k + 1);
-      s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
-      s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
-    }
-#pragma unroll
-    for (int i = 8; i < 16; i++) s[i] = 0;
-    p2_permute<F>(s);
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      buf[8 * tid + i] = s[i];
-      A.tree[8 * k + i] = s[i];
-    }
-  }
-  __syncthreads();
-  cta_reduce<F>(buf, here, 0, base, A.tree, A.log_leaves);
-  // promotion: the last CTA of each group of 256 nodes carries on
-  uint32_t lvl = 31 - __clz(here);
-  uint64_t idx = blockIdx.x, items = n_leaves >> lvl;
-  uint32_t coff = 0;
-  while (items > 1) {
-    const uint64_t group = idx / kFriRoundCta;
-    const uint32_t gsize = items < kFriRoundCta ? (uint32_t)items : kFriRoundCta;
-    __threadfence();  // this CTA's nodes are visible before its count
-    __syncthreads();
-    if (tid == 0) {
-      const uint32_t prev = atomicAdd(A.counters + coff + group, 1u);
-      s_last = prev == gsize - 1;
-      if (s_last) A.counters[coff + group] = 0;  // ready for the next round's launch
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const uint32_t* src = A.tree + layer_words(A.log_leaves, lvl) + group * kFriRoundCta * 8;
-    for (uint32_t i = tid; i < gsize * 8; i += blockDim.x) buf[i] = __ldcg(src + i);
-    __syncthreads();
-    cta_reduce<F>(buf, gsize, lvl, group * kFriRoundCta, A.tree, A.log_leaves);
-    lvl += 31 - __clz(gsize);
-    coff += (uint32_t)((items + kFriRoundCta - 1) / kFriRoundCta);
-    idx = group;
-    items = (items + kFriRoundCta - 1) / kFriRoundCta;
-  }
-  if (A.ch && tid == 0) {
-    for (int i = 0; i < 8; i++) ch_observe<F>(A.ch, buf[i]);
-    for (int i = 0; i < 4; i++) A.beta_out[i] = ch_sample<F>(A.ch);
-  }
-}
-
-// Counters one round needs (one per promotion group at every height).
-uint32_t fri_round_counters(uint32_t log_leaves) {
-  uint64_t items = 1ull << (log_leaves > 8 ? log_leaves - 8 : 0);
-  uint32_t n = 0;
-  while (items > 1) {
-    items = (items + kFriRoundCta - 1) / kFriRoundCta;
-    n += (uint32_t)items;
-  }
-  return n;
-}
-
-cudaError_t launch_fri_round(int field, bool fold, const uint32_t* cw_in, const uint32_t* beta_in,
-                             const uint32_t* inject, uint32_t* cw_out, uint32_t* tree, uint32_t log_leaves,
-                             uint32_t* counters, DevChallenger* ch, uint32_t* beta_out, TwiddleTables tw,
-                             cudaStream_t st) {
-  FriRoundArgs A{cw_in, beta_in, inject, cw_out, tree, counters, ch, beta_out, log_leaves};
-  const uint64_t n = 1ull << log_leaves;
-  const unsigned grid = (unsigned)((n + kFriRoundCta - 1) / kFriRoundCta);
-  if (field == 0) {
-    if (fold) k_fri_round<KoalaBear, true><<<grid, kFriRoundCta, 0, st>>>(A, tw);
-    else k_fri_round<KoalaBear, false><<<grid, kFriRoundCta, 0, st>>>(A, tw);
-  } else {
-    if (fold) k_fri_round<BabyBear, true><<<grid, kFriRoundCta, 0, st>>>(A, tw);
-    else k_fri_round<BabyBear, false><<<grid, kFriRoundCta, 0, st>>>(A, tw);
-  }
-  return cudaGetLastError();
-}
-
 // Seven compression levels in one launch: CTA c reduces input nodes
 // [128 c, 128 c + 128) of a level of n_in nodes to one node, four lanes per
 // state, and writes every level it computes to the tree (level l + 1 follows

@@ -12,7 +12,7 @@ import pytest
 
 from pico_b200 import PicoError, TwoAdicDomain, TwoAdicFriPcs
 from pico_b200 import fields as F
-from pico_b200.quotient import ConstraintBuilder, compute_quotient_values
+from pico_b200.quotient import OPS, ConstraintBuilder, compute_quotient_values
 
 pytestmark = pytest.mark.gpu
 FIELDS = [0, 1]
@@ -164,12 +164,13 @@ def test_device_output_and_refusals(gpu, orc):
     assert (out.cpu().numpy().view(np.uint32) == want).all()
     with pytest.raises(PicoError):  # quotient domain taller than the committed LDE (blowup 1)
         compute_quotient_values(gpu, prog, logn, 2, (pd, 0), alpha=alpha)
+    k = int(np.nonzero(prog[:, 0] == OPS["MAIN"])[0][0])
     bad = prog.copy()
-    bad[0, 2] = 5  # main column beyond the width
+    bad[k, 2] = 5  # main column beyond the width
     with pytest.raises(PicoError):
         compute_quotient_values(gpu, bad, logn, log_qd, (pd, 0), alpha=alpha)
     bad = prog.copy()
-    bad[0, 1] = 64  # base register beyond the register file
+    bad[k, 1] = 64  # base register beyond the register file
     with pytest.raises(PicoError):
         compute_quotient_values(gpu, bad, logn, log_qd, (pd, 0), alpha=alpha)
     pd.release()
