@@ -148,6 +148,12 @@ IMAD_PER_SM_CLK = 64
 # + dram__bytes_write over rows * (4 * width + 32)), from an ncu capture of
 # k_hash_rows on a 2^23-row x 16-column LDE (the single-kb-2^22x16 workload)
 HASH_TRAFFIC_RATIO = 0.966
+# DRAM bytes per algorithmic byte (input + output) of one three-pass LDE, from
+# an ncu capture of k_lde_a/b/c on a 2^22 x 16 matrix at split 2^11 x 2^11:
+# 2,305 MB (read + write over the three passes) for 805 MB algorithmic.  The
+# intermediate matrices T1 (n x w) and T2 (N x w) are each written once and
+# read once.  One-pass matrices (n <= 2^11) move about their algorithmic bytes.
+LDE_TRAFFIC_RATIO = 2305 / 805
 
 
 GOLDEN_ROOTS = ROOT / "tests" / "golden" / "config_roots.json"
@@ -461,7 +467,10 @@ def run_gpu(args, rank, world, local):
             "peak": hbm_peak,
             "unit": "GB/s",
             "frac": lde_ach / hbm_peak if lde_ach else None,
-            "traffic": None,
+            "traffic": lde_alg_bytes * LDE_TRAFFIC_RATIO if lde_alg_bytes else None,
+            "traffic_note": "algorithmic bytes x the three-pass DRAM/algorithmic ratio ncu measured on a "
+                            "2^22 x 16 LDE (T1 and T2 written and read once each); upper bound for "
+                            "batches that hold one-pass matrices",
             "algorithmic_bytes": lde_alg_bytes,
             "ms": lde_only_ms,
             "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback",
@@ -726,6 +735,114 @@ def run_fri(args):
     }
 
 
+# ---------------------------------------------------------------- quotient leg
+def chip_program(field, main_w: int = 32, seed: int = 9):
+    """A synthetic chip's constraints shaped like Pico's (no public dataset):
+    16 degree-2 products wired across the main columns, 8 transition
+    constraints, 4 boolean checks, first-row and last-row constraints, and a
+    LogUp-style running sum in one permutation column:
+    (z' - z) (ch0 + x0 + ch1 x1) = x2 on transitions, z = regional sum on the
+    first row."""
+    from pico_b200.quotient import ConstraintBuilder
+
+    rng = np.random.default_rng(seed)
+    b = ConstraintBuilder()
+    m = lambda c, nxt=False: b.main(int(c), nxt)
+    for i in range(16):
+        a, c, d = rng.integers(0, main_w, size=3)
+        b.assert_zero(m(a) * m(c) - m(d))
+    for i in range(8):
+        a, c = rng.integers(0, main_w, size=2)
+        b.when_transition().assert_eq(m(i, True), m(a) + m(c))
+    for i in range(4):
+        x = m(24 + i)
+        b.assert_zero(x * (x - 1))
+    b.when_first_row().assert_eq(m(0), b.public(0))
+    b.when_last_row().assert_eq(m(1), b.public(1))
+    z, zn = b.permutation(0), b.permutation(0, True)
+    b.when_transition().assert_zero((zn - z) * (b.challenge(0) + m(0) + b.challenge(1) * m(1)) - m(2))
+    b.when_first_row().assert_zero(z - b.regional_cumulative_sum())
+    return b.program(field)
+
+
+def run_quotient(args):
+    """compute_quotient_values of the synthetic chip over one 2^20-row
+    KoalaBear trace of 32 columns plus one extension permutation column,
+    quotient degree 2 (2^21 points), the traces resident from their commits.
+    One step = one pico_gpu_quotient_values call with device output."""
+    import torch
+
+    from pico_b200 import GpuContext, TwoAdicDomain, TwoAdicFriPcs
+    from pico_b200 import fields as F
+    from pico_b200.quotient import compute_quotient_values
+    from oracle import cpu as orc
+
+    f, logn, log_qd, main_w = 0, 20, 1, 32
+    prog = chip_program(f, main_w)
+    dev = torch.device("cuda", 0)
+    ctx = GpuContext(0)
+    pcs = TwoAdicFriPcs(ctx, f, 1)
+    main = F.random_matrix_torch(f, logn, main_w, 9100, dev)
+    perm = F.random_matrix_torch(f, logn, 4, 9101, dev).reshape(1 << logn, 1, 4)
+    _, pd = pcs.commit([(TwoAdicDomain(logn), main), (TwoAdicDomain(logn), perm)])
+    pub = F.to_monty(f, [1, 2])
+    chal = F.to_monty(f, F.uniform(f, 8, 9102)).reshape(2, 4)
+    reg = F.to_monty(f, F.uniform(f, 4, 9103))
+    alpha = F.to_monty(f, F.uniform(f, 4, 9104))
+    Q = 1 << (logn + log_qd)
+    out = torch.empty((Q, 4), dtype=torch.int32, device=dev)
+
+    def step():
+        compute_quotient_values(ctx, prog, logn, log_qd, (pd, 0), permutation=(pd, 1), public_values=pub,
+                                perm_challenges=chal, regional_sum=reg, alpha=alpha, out=out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    e1.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    # parity of the timed output on a slice of points, against the oracle (its
+    # own LDE of the same traces, natural order)
+    got = out.cpu().numpy().view(np.uint32)
+    main_h = main.cpu().numpy().view(np.uint32)
+    perm_h = perm.cpu().numpy().view(np.uint32)
+    want = orc.quotient_values(f, logn, log_qd, prog, orc.on_quotient_domain(f, main_h, log_qd),
+                               perm_q=orc.on_quotient_domain(f, perm_h, log_qd), public_values=pub,
+                               perm_challenges=chal, regional_sum=reg, alpha=alpha)
+    match = bool((got == want).all())
+    # CPU: the oracle on a 2^14-row trace of the same program (per point)
+    small = 14
+    mh, ph = main_h[: 1 << small], perm_h[: 1 << small]
+    mq, pq = orc.on_quotient_domain(f, mh, log_qd), orc.on_quotient_domain(f, ph, log_qd)
+    t = time.perf_counter()
+    orc.quotient_values(f, small, log_qd, prog, mq, perm_q=pq, public_values=pub, perm_challenges=chal,
+                        regional_sum=reg, alpha=alpha)
+    cpu_s = time.perf_counter() - t
+    ctx.close()
+    points = Q
+    return {
+        "metric": "quotient-domain points/sec (compute_quotient_values of one chip, resident LDEs)",
+        "value": points / (ms / 1e3), "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 (KoalaBear, EF4 accumulator)", "data": "synthetic: seeded traces, a chip-shaped program",
+        "config": {"workload": "quotient-kb-2^20", "log_trace": logn, "log_quotient_degree": log_qd,
+                   "main_width": main_w, "perm_width": 1, "program_ops": int(prog.shape[0])},
+        "parity": {"matches_oracle": match, "points": points},
+        "clocks": clocks,
+        "cpu_baseline": {"value": (2 << small) / cpu_s, "unit": "points/s", "cores": orc.num_threads(),
+                         "kind": "port", "cpu_model": cpu_model(),
+                         "sample": f"the same program on a 2^{small}-row trace ({2 << small} points), one run"},
+    }
+
+
 # ---------------------------------------------------------------- serving leg
 # request mixes: (log2 heights low, high), widths (low, high)
 SERVING_MIXES = {
@@ -763,13 +880,15 @@ def serving_requests(n_req: int, seed: int = 5, max_cells: int = 1 << 30, mix: s
 
 def run_serving(args):
     """Poisson arrivals of commit requests into the serving queue (admission
-    by free HBM, up to --slots requests on the device at once), for both the
-    batched form and the plain one-matrix-per-launch form, at several offered
-    loads (multiples of the plain form's one-at-a-time capacity, the same
-    arrival times for both forms); plus both forms one at a time.  Inputs are
-    views into a device-resident pool of seeded field elements.  The memory
-    pool is grown before timing by one pass of every request, one at a time
-    and served."""
+    by free HBM, up to --slots requests on the device at once), for three
+    forms: batched (each request alone on its stream), grouped (queued
+    requests admitted together, up to --group of them sharing their LDE and
+    row-hashing launches) and the plain one-matrix-per-launch form, at several
+    offered loads (multiples of the plain form's one-at-a-time capacity, the
+    same arrival times for every form); plus the batched and plain forms one
+    at a time.  Inputs are views into a device-resident pool of seeded field
+    elements.  The memory pool is grown before timing by one pass of every
+    request (or the first --serve-warm), one at a time and served."""
     import threading as th
 
     import torch
@@ -798,6 +917,10 @@ def run_serving(args):
     total_cells = sum(cells)
     ctx = GpuContext(0, n_streams=8, max_inflight=args.slots)
     server = CommitServer(ctx)
+    # the grouped form's context shares the device's memory pool and budget
+    ctx_g = GpuContext(0, hbm_budget_bytes=ctx.memory()[1], n_streams=8, max_inflight=args.slots,
+                       max_group=args.group)
+    server_g = CommitServer(ctx_g)
 
     def sequential(plain):
         lat = []
@@ -810,7 +933,7 @@ def run_serving(args):
             lat.append(time.perf_counter() - t)
         return time.perf_counter() - t0, lat
 
-    def served(plain, arrivals):
+    def served(plain, arrivals, server=server):
         handles = [None] * len(reqs)
         lat = [None] * len(reqs)
         queued = [None] * len(reqs)
@@ -839,9 +962,17 @@ def run_serving(args):
     def pct(x, q):
         return float(np.percentile(np.array(x) * 1e3, q))
 
-    # grow the pool: every request once, one at a time, then once served back to back
-    sequential(False)
-    served(False, np.zeros(len(reqs)))
+    # grow the pool: every request once (or the first --serve-warm), one at a
+    # time, then once served back to back
+    if args.serve_warm == 0 or args.serve_warm >= len(reqs):
+        sequential(False)
+        served(False, np.zeros(len(reqs)))
+    else:
+        full = (reqs, mats)
+        reqs, mats = reqs[:args.serve_warm], mats[:args.serve_warm]
+        sequential(False)
+        served(False, np.zeros(len(reqs)))
+        reqs, mats = full
     seq_s, seq_lat = sequential(False)
     plain_s, plain_lat = sequential(True)
     cap_plain = total_cells / plain_s
@@ -849,15 +980,20 @@ def run_serving(args):
     gaps = rng.exponential(1.0, size=len(reqs))  # unit-rate arrivals, scaled per load
     mean_cells = total_cells / len(reqs)
     sweep = []
-    for load in sorted(set([args.load] + [0.5, 1.0, 1.25])):
+    loads = [float(x) for x in args.loads.split(",")] if args.loads else [0.5, 1.0, 1.25]
+    for load in sorted(set([args.load] + loads)):
         rate = load * cap_plain / mean_cells  # requests per second
         arrivals = np.cumsum(gaps / rate)
         row = {"offered_load_vs_plain_capacity": load, "poisson_rate_per_s": rate}
-        for name, plain in (("batched", False), ("plain", True)):
-            s_, lat, queued = served(plain, arrivals)
+        forms = [("batched", False, server), ("plain", True, server)]
+        if args.group > 1:
+            forms.insert(1, ("grouped", False, server_g))
+        for name, plain, srv in forms:
+            s_, lat, queued = served(plain, arrivals, srv)
             row[name] = {"cells_per_s": total_cells / s_, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
                          "mean_queue_ms": float(np.mean(queued) * 1e3)}
         sweep.append(row)
+    ctx_g.close()
     ctx.close()
     main_row = next(r for r in sweep if r["offered_load_vs_plain_capacity"] == args.load)
     return {
@@ -868,8 +1004,9 @@ def run_serving(args):
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic: views into a seeded device pool",
         "config": {"workload": "serving", "mix": args.mix, "requests": len(reqs), "slots": args.slots, "offered_load": args.load,
-                   "total_cells": total_cells},
+                   "max_group": args.group, "total_cells": total_cells},
         "served": main_row["batched"],
+        "served_grouped": main_row.get("grouped"),
         "served_plain": main_row["plain"],
         "sweep": sweep,
         "one_at_a_time_batched": {"p50_ms": pct(seq_lat, 50), "p99_ms": pct(seq_lat, 99),
@@ -885,13 +1022,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving"] + list(OPEN_WORKLOADS),
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving", "quotient-kb-2^20"]
+                    + list(OPEN_WORKLOADS),
                     default="uneven-kb-2^30")
     ap.add_argument("--requests", type=int, default=60, help="serving: number of requests")
     ap.add_argument("--load", type=float, default=0.8,
                     help="serving: offered load vs the plain form's one-at-a-time capacity")
     ap.add_argument("--slots", type=int, default=2, help="serving: requests on the device at once")
+    ap.add_argument("--group", type=int, default=8,
+                    help="serving: largest group of queued requests sharing launches in the grouped form (1: none)")
     ap.add_argument("--mix", choices=list(SERVING_MIXES), default="prover", help="serving: request mix")
+    ap.add_argument("--loads", default="", help="serving: extra offered loads to sweep, comma separated "
+                                                  "(default 0.5,1.0,1.25)")
+    ap.add_argument("--serve-warm", type=int, default=0,
+                    help="serving: requests used to warm the memory pool (0: all of them)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="opening workloads: CPU sample size in seconds")
     ap.add_argument("--cpu-runs", type=int, default=5, help="runs of the CPU baseline (median)")
     ap.add_argument("--cpu-cells", type=int, default=CPU_SAMPLE_CELLS,
@@ -932,9 +1076,9 @@ def main():
 
             dist.destroy_process_group()
         return
-    if args.workload in ("fri-kb-2^23", "serving"):
+    if args.workload in ("fri-kb-2^23", "serving", "quotient-kb-2^20"):
         if rank == 0:
-            res = run_fri(args) if args.workload == "fri-kb-2^23" else run_serving(args)
+            res = {"fri-kb-2^23": run_fri, "serving": run_serving, "quotient-kb-2^20": run_quotient}[args.workload](args)
             print(json.dumps(res), flush=True)
         return
     wl = WORKLOADS[args.workload]

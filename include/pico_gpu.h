@@ -87,7 +87,10 @@ typedef struct {
   uint32_t n_streams;        /* device streams for concurrent requests; 0 = 8 */
   uint32_t flags;
   uint32_t max_inflight;     /* serving: requests on the device at once; 0 = n_streams */
-  uint32_t reserved[5];
+  uint32_t max_group;        /* serving: queued requests admitted together as one group that shares its
+                                LDE and row-hashing launches (batched device-input requests of one field);
+                                0 or 1 = each request alone, at most 16 */
+  uint32_t reserved[4];
 } pico_config;
 
 /* Device-side timing and work counts of one commit, from CUDA events recorded

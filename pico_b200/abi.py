@@ -67,7 +67,8 @@ class Config(C.Structure):
         ("n_streams", C.c_uint32),
         ("flags", C.c_uint32),
         ("max_inflight", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("max_group", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 

@@ -415,6 +415,7 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
   ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
   const uint32_t ns = (cfg && cfg->n_streams) ? cfg->n_streams : 8;
   ctx->max_inflight = (cfg && cfg->max_inflight) ? std::min(cfg->max_inflight, ns) : ns;
+  ctx->max_group = (cfg && cfg->max_group) ? std::min<uint32_t>(cfg->max_group, kMaxGroup) : 1;
   for (uint32_t i = 0; i < ns; i++) {
     cudaStream_t st, cst;
     if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;
@@ -688,6 +689,44 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   return PICO_OK;
 }
 
+// The compression levels of a commit's tree on st: `layers` holds the leaf
+// digests; inj[g] (g >= 1) the row digests of height group g, injected at
+// the level its height meets.  *root receives the root's address.
+pico_status enqueue_tree(const CommitPlan& plan, uint32_t* layers, const std::vector<uint32_t*>& inj,
+                         cudaStream_t st, uint64_t* launches, uint32_t** root) {
+  pico_status s;
+  const int field = plan.field;
+  const uint32_t log_max = plan.log_max;
+  const uint32_t G = (uint32_t)plan.groups.size();
+  uint32_t* layer = layers;
+  uint32_t next_group = 1;
+  for (uint32_t lvl = 1; lvl <= log_max;) {
+    const uint64_t len = 1ull << (log_max - lvl);  // nodes of the level being made
+    if (2 * len <= (1u << 15) && 2 * len >= kSubtreeIn) {
+      // the narrow levels seven at a time (k_subtree_quad), with the injected
+      // rows of the groups whose heights they meet
+      SubtreeInj si{};
+      for (uint32_t l = 0; l < 7; l++)
+        if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - (lvl + l))
+          si.digests[l] = inj[next_group++];
+      if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)(2 * len), si, st), "compression"))) return s;
+      *launches += 1;
+      for (uint32_t l = 0; l < 7; l++) layer += ((2 * len) >> l) * 8;
+      lvl += 7;
+      continue;
+    }
+    uint32_t* next = layer + (2 * len) * 8;
+    const uint32_t* d = nullptr;
+    if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - lvl) d = inj[next_group++];
+    if ((s = cuda_status(launch_compress(field, layer, next, len, d, st), "compression"))) return s;
+    *launches += 1;
+    layer = next;
+    lvl++;
+  }
+  *root = layer;
+  return PICO_OK;
+}
+
 // Enqueue a whole commit: LDEs and Poseidon2 on `st`, host -> device input
 // copies on `cst`, so copies overlap the compute.  On success `c` holds the
 // resident buffers and `scratch` the buffers to free once `st` has passed
@@ -698,8 +737,35 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
 // Host inputs are copied shortest group first, so the LDEs and row digests
 // of the short groups run while the tallest group is still in transit; the
 // tallest group's LDE, its leaf hashing and the compression levels come last.
-pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
-                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
+// Matrices of height group gi with columns (width-0 matrices add nothing to a row).
+static uint32_t nonzero_mats(const CommitPlan& plan, uint32_t gi) {
+  uint32_t c = 0;
+  for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) c += plan.mats[k].w != 0;
+  return c;
+}
+
+// The buffers and descriptors of one commit, made by setup_commit.
+struct CommitSetup {
+  std::vector<bool> chained;               // per height group: hashed matrix by matrix (resumable sponge)
+  std::vector<LdeMat> hm;                  // per planned matrix (extended commits)
+  std::vector<const uint32_t*> leaves;     // what the tree hashes, per planned matrix
+  std::vector<uint32_t*> inj;              // per height group g >= 1: its row digests
+  uint32_t* state = nullptr;               // row states of chained groups
+  std::vector<cudaEvent_t> arrived;        // host inputs: matrix k (and all before it) on the device
+  CommitSetup() = default;
+  CommitSetup(const CommitSetup&) = delete;
+  CommitSetup& operator=(const CommitSetup&) = delete;
+  ~CommitSetup() {
+    for (auto e : arrived)
+      if (e) cudaEventDestroy(e);  // released once the device has passed them
+  }
+};
+
+// Open a commit on st: its events, its device buffers (resident ones into c,
+// scratch into `scratch`), the host -> device input copies on cst, and the
+// LDE and row-group descriptors over them.
+static pico_status setup_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
+                                pico_commit* c, std::vector<void*>& scratch, CommitSetup& cs) {
   pico_status s;
   const int field = plan.field;
   const uint32_t n = (uint32_t)plan.mats.size();
@@ -755,15 +821,11 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   // time as each arrives (resumable sponge), the row states kept in `state`
   // between matrices; its size is the largest such group's rows x 16 words.
   // The plain form hashes matrix by matrix too (one launch per matrix).
-  auto nonzero = [&](uint32_t gi) {
-    uint32_t c = 0;
-    for (uint32_t k = plan.groups[gi].first; k < plan.groups[gi].second; k++) c += plan.mats[k].w != 0;
-    return c;
-  };
-  std::vector<bool> chained(G, false);
+  std::vector<bool>& chained = cs.chained;
+  chained.assign(G, false);
   uint64_t rows_max = 0;
   for (uint32_t gi = 0; gi < G; gi++) {
-    chained[gi] = (copy_in || plan.plain) && nonzero(gi) >= 2;
+    chained[gi] = (copy_in || plan.plain) && nonzero_mats(plan, gi) >= 2;
     if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
   }
   const uint32_t nb = 1u << plan.log_b;
@@ -841,11 +903,8 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
 
   // ---- host -> device copies on cst: shortest group first, each group's
   // matrices in commit order; arrived[k] marks matrix k (and all before it) ----
-  std::vector<cudaEvent_t> arrived(n, nullptr);
-  auto destroy_events = [&]() {
-    for (auto e : arrived)
-      if (e) cudaEventDestroy(e);  // released once the device has passed them
-  };
+  std::vector<cudaEvent_t>& arrived = cs.arrived;
+  arrived.assign(n, nullptr);
   if ((s = cuda_status(cudaEventRecord(c->ev[5], st), "event"))) return s;
   if (copy_in) {
     if ((s = cuda_status(cudaStreamWaitEvent(cst, c->ev[5], 0), "copy stream wait"))) return s;
@@ -854,36 +913,24 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
         if (in_bytes[k] &&
             (s = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(dev_in[k]), plan.mats[k].src, in_bytes[k],
                                              cudaMemcpyHostToDevice, cst),
-                             "input copy"))) {
-          destroy_events();
+                             "input copy")))
           return s;
-        }
         cudaEvent_t e;
-        if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) {
-          destroy_events();
-          return s;
-        }
+        if ((s = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) return s;
         arrived[k] = e;
-        if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) {
-          destroy_events();
-          return s;
-        }
+        if ((s = cuda_status(cudaEventRecord(e, cst), "event"))) return s;
       }
     }
-    if ((s = cuda_status(cudaEventRecord(c->ev[6], cst), "event"))) {
-      destroy_events();
-      return s;
-    }
+    if ((s = cuda_status(cudaEventRecord(c->ev[6], cst), "event"))) return s;
   } else {
     if ((s = cuda_status(cudaEventRecord(c->ev[6], st), "event"))) return s;
   }
 
-  if (!packed && (s = alloc_through(order.size()))) {
-    destroy_events();
-    return s;
-  }
-  std::vector<LdeMat> hm(plan.extend ? n : 0);
-  std::vector<const uint32_t*> leaves(n, nullptr);  // what the tree hashes, per planned matrix
+  if (!packed && (s = alloc_through(order.size()))) return s;
+  std::vector<LdeMat>& hm = cs.hm;
+  hm.assign(plan.extend ? n : 0, LdeMat{});
+  std::vector<const uint32_t*>& leaves = cs.leaves;
+  leaves.assign(n, nullptr);
   if (plan.extend) {
     uint32_t* pw = in_scr(ix_pw);  // all (matrix, coset) power tables
     for (uint32_t k = 0; k < n; k++) {
@@ -922,7 +969,8 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
   }
   c->layers = in_res(ix_layers);
   // digests of the rows of every shorter height group, injected at its level
-  std::vector<uint32_t*> inj(G, nullptr);
+  std::vector<uint32_t*>& inj = cs.inj;
+  inj.assign(G, nullptr);
   if (inj_words) {
     uint64_t off = 0;
     for (uint32_t g = 1; g < G; g++) {
@@ -930,7 +978,80 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       off += 8ull << plan.mats[plan.groups[g].first].log_N;
     }
   }
-  uint32_t* state = ix_state == kNone ? nullptr : in_scr(ix_state);
+  cs.state = ix_state == kNone ? nullptr : in_scr(ix_state);
+  return PICO_OK;
+}
+
+// Phase brackets of a commit's timings (pico_commit::phases) on st.
+static pico_status phase_begin(pico_commit* c, int kind, cudaStream_t st) {
+  pico_commit::Phase ph;
+  ph.kind = kind;
+  pico_status r;
+  if ((r = cuda_status(cudaEventCreate(&ph.begin), "event"))) return r;
+  if ((r = cuda_status(cudaEventCreate(&ph.end), "event"))) {
+    cudaEventDestroy(ph.begin);
+    return r;
+  }
+  c->phases.push_back(ph);
+  return cuda_status(cudaEventRecord(ph.begin, st), "event");
+}
+static pico_status phase_end(pico_commit* c, cudaStream_t st) {
+  return cuda_status(cudaEventRecord(c->phases.back().end, st), "event");
+}
+
+// Row digests of several height groups, gathered into k_hash_groups
+// launches of up to kBatchGroups groups and kBatchSegs segments.
+struct HashBatcher {
+  GroupBatch b;
+  HashBatcher() { memset(&b, 0, sizeof b); }
+  bool empty() const { return b.n_groups == 0; }
+  // Whether the rows of planned matrices [first, last) still fit this launch.
+  bool fits(const CommitPlan& plan, uint32_t first, uint32_t last) const {
+    uint32_t segs = 0;
+    for (uint32_t k = first; k < last; k++) segs += plan.mats[k].w != 0;
+    return b.n_groups < (uint32_t)kBatchGroups && b.n_segs + segs <= (uint32_t)kBatchSegs;
+  }
+  // Add the group of planned matrices [first, last) (rows each, data at
+  // leaves[k]); its digests go to out.  Call only when fits().
+  void add(const CommitPlan& plan, const std::vector<const uint32_t*>& leaves, uint32_t first, uint32_t last,
+           uint64_t rows, uint32_t* out) {
+    const uint32_t g = b.n_groups;
+    b.seg_begin[g] = b.n_segs;
+    uint32_t width = 0;
+    for (uint32_t k = first; k < last; k++) {
+      if (plan.mats[k].w == 0) continue;
+      b.segs[b.n_segs].ptr = leaves[k];
+      b.segs[b.n_segs].width = plan.mats[k].w;
+      b.n_segs++;
+      width += plan.mats[k].w;
+    }
+    b.seg_begin[g + 1] = b.n_segs;
+    b.width[g] = width;
+    b.out[g] = out;
+    b.row_end[g] = (g ? b.row_end[g - 1] : 0ull) + rows;
+    b.n_groups = g + 1;
+  }
+  pico_status launch(int field, cudaStream_t st, unsigned block) {
+    const pico_status r = cuda_status(launch_hash_groups(field, b, st, block), "row hashing");
+    memset(&b, 0, sizeof b);
+    return r;
+  }
+};
+
+pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
+                           pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host) {
+  CommitSetup cs;
+  pico_status s = setup_commit(ctx, plan, st, cst, c, scratch, cs);
+  if (s) return s;
+  const int field = plan.field;
+  const uint32_t G = (uint32_t)plan.groups.size();
+  const bool copy_in = !plan.input_device;
+  const std::vector<bool>& chained = cs.chained;
+  const std::vector<LdeMat>& hm = cs.hm;
+  const std::vector<const uint32_t*>& leaves = cs.leaves;
+  const std::vector<uint32_t*>& inj = cs.inj;
+  const std::vector<cudaEvent_t>& arrived = cs.arrived;
+  uint32_t* const state = cs.state;
 
   // ---- compute on st, one height group at a time ----
   // Shortest group first (the order host copies arrive in): its LDE, then
@@ -968,55 +1089,26 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     return cuda_status(launch_lde(field, mats.data(), (uint32_t)mats.size(), tw, st, &c->stats.launches),
                        "LDE launch");
   };
-  auto begin_phase = [&](int kind) -> pico_status {
-    pico_commit::Phase ph;
-    ph.kind = kind;
-    pico_status r;
-    if ((r = cuda_status(cudaEventCreate(&ph.begin), "event"))) return r;
-    if ((r = cuda_status(cudaEventCreate(&ph.end), "event"))) {
-      cudaEventDestroy(ph.begin);
-      return r;
-    }
-    c->phases.push_back(ph);
-    return cuda_status(cudaEventRecord(ph.begin, st), "event");
-  };
-  auto end_phase = [&]() { return cuda_status(cudaEventRecord(c->phases.back().end, st), "event"); };
+  auto begin_phase = [&](int kind) { return phase_begin(c, kind, st); };
+  auto end_phase = [&]() { return phase_end(c, st); };
   // The batched form hashes the rows of the shorter groups (those hashed in
   // one pass) together: each is added to `batch` after its LDE, and one
   // launch before the tallest group computes all their digests.  A group
   // with few rows is a few thousand short sponges, latency-bound on its own.
-  GroupBatch batch;
-  memset(&batch, 0, sizeof batch);
+  HashBatcher batch;
   auto flush_batch = [&]() -> pico_status {
-    if (!batch.n_groups) return PICO_OK;
+    if (batch.empty()) return PICO_OK;
     pico_status r;
     if ((r = begin_phase(pico_commit::kRows))) return r;
-    r = cuda_status(launch_hash_groups(field, batch, st, ctx->hash_block[field]), "row hashing");
+    r = batch.launch(field, st, ctx->hash_block[field]);
     c->stats.launches += 1;
     if (!r) r = end_phase();
-    memset(&batch, 0, sizeof batch);
     return r;
   };
   auto add_to_batch = [&](uint32_t first, uint32_t last, uint64_t rows, uint32_t* out) -> pico_status {
-    uint32_t segs = 0;
-    for (uint32_t k = first; k < last; k++) segs += plan.mats[k].w != 0;
-    if (batch.n_groups == (uint32_t)kBatchGroups || batch.n_segs + segs > (uint32_t)kBatchSegs)
+    if (!batch.fits(plan, first, last))
       if (pico_status r = flush_batch()) return r;
-    const uint32_t g = batch.n_groups;
-    batch.seg_begin[g] = batch.n_segs;
-    uint32_t width = 0;
-    for (uint32_t k = first; k < last; k++) {
-      if (plan.mats[k].w == 0) continue;
-      batch.segs[batch.n_segs].ptr = leaves[k];
-      batch.segs[batch.n_segs].width = plan.mats[k].w;
-      batch.n_segs++;
-      width += plan.mats[k].w;
-    }
-    batch.seg_begin[g + 1] = batch.n_segs;
-    batch.width[g] = width;
-    batch.out[g] = out;
-    batch.row_end[g] = (g ? batch.row_end[g - 1] : 0ull) + rows;
-    batch.n_groups = g + 1;
+    batch.add(plan, leaves, first, last, rows, out);
     return PICO_OK;
   };
   uint32_t* layer = c->layers;
@@ -1042,7 +1134,7 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
       if (s || (s = end_phase())) break;
       continue;
     }
-    uint32_t cols = 0, left = nonzero(gi);
+    uint32_t cols = 0, left = nonzero_mats(plan, gi);
     for (uint32_t k = first; k < last && !s; k++) {
       if (plan.mats[k].w == 0) continue;
       left--;
@@ -1060,36 +1152,93 @@ pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t s
     }
   }
   if (!s) s = flush_batch();
-  destroy_events();
   if (s) return s;
   if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;
-  uint32_t next_group = 1;
-  for (uint32_t lvl = 1; lvl <= log_max;) {
-    const uint64_t len = 1ull << (log_max - lvl);  // nodes of the level being made
-    if (2 * len <= (1u << 15) && 2 * len >= kSubtreeIn) {
-      // the narrow levels seven at a time (k_subtree_quad), with the injected
-      // rows of the groups whose heights they meet
-      SubtreeInj si{};
-      for (uint32_t l = 0; l < 7; l++)
-        if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - (lvl + l))
-          si.digests[l] = inj[next_group++];
-      if ((s = cuda_status(launch_subtree(field, layer, (uint32_t)(2 * len), si, st), "compression"))) return s;
-      c->stats.launches += 1;
-      for (uint32_t l = 0; l < 7; l++) layer += ((2 * len) >> l) * 8;
-      lvl += 7;
-      continue;
-    }
-    uint32_t* next = layer + (2 * len) * 8;
-    const uint32_t* d = nullptr;
-    if (next_group < G && plan.mats[plan.groups[next_group].first].log_N == log_max - lvl) d = inj[next_group++];
-    if ((s = cuda_status(launch_compress(field, layer, next, len, d, st), "compression"))) return s;
-    c->stats.launches += 1;
-    layer = next;
-    lvl++;
-  }
+  if ((s = enqueue_tree(plan, layer, inj, st, &c->stats.launches, &layer))) return s;
   if ((s = cuda_status(cudaEventRecord(c->ev[4], st), "event"))) return s;
   if (root_host)
     if ((s = cuda_status(cudaMemcpyAsync(root_host, layer, 32, cudaMemcpyDeviceToHost, st), "root copy"))) return s;
+  return PICO_OK;
+}
+
+// Several commits of one field on st, admitted together by the serving
+// path: their LDEs share launches (one per pass and sub-transform length for
+// every kLdeBatch matrices, shortest traces first so that equal lengths share
+// a batch), the rows of all their height groups, the tallest (the leaves)
+// included, share k_hash_groups launches, and each commit's compression
+// levels follow on their own, its root copied to root_host[i].  Every commit's
+// LDE and hashing phases bracket the shared launches, and its launch count
+// includes them.  Inputs must be device pointers (no copies to overlap) and
+// the commits extended in the batched form.
+pico_status enqueue_commit_group(pico_ctx* ctx, const std::vector<const CommitPlan*>& plans, cudaStream_t st,
+                                 const std::vector<pico_commit*>& commits, std::vector<void*>& scratch,
+                                 const std::vector<uint32_t*>& root_host) {
+  const size_t K = plans.size();
+  if (K == 0 || commits.size() != K || root_host.size() != K) {
+    set_error("commit group: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const int field = plans[0]->field;
+  for (const CommitPlan* p : plans)
+    if (p->field != field || !p->input_device || !p->extend || p->plain) {
+      set_error("commit group: members must share the field and be extended batched commits of device inputs");
+      return PICO_ERR_INVALID_ARG;
+    }
+  pico_status s;
+  std::vector<std::unique_ptr<CommitSetup>> cs(K);
+  for (size_t i = 0; i < K; i++) {
+    cs[i].reset(new CommitSetup());
+    if ((s = setup_commit(ctx, *plans[i], st, st, commits[i], scratch, *cs[i]))) return s;
+  }
+  auto phases = [&](bool begin, int kind) -> pico_status {
+    for (size_t i = 0; i < K; i++)
+      if (pico_status r = begin ? phase_begin(commits[i], kind, st) : phase_end(commits[i], st)) return r;
+    return PICO_OK;
+  };
+  // LDEs of every member's matrices with columns
+  std::vector<LdeMat> lde;
+  for (size_t i = 0; i < K; i++)
+    for (const LdeMat& m : cs[i]->hm)
+      if (m.w) lde.push_back(m);
+  std::stable_sort(lde.begin(), lde.end(), [](const LdeMat& a, const LdeMat& b) { return a.log_n < b.log_n; });
+  uint64_t shared = 0;
+  if ((s = phases(true, pico_commit::kLde))) return s;
+  if (!lde.empty() &&
+      (s = cuda_status(launch_lde(field, lde.data(), (uint32_t)lde.size(), twiddles(ctx, field), st, &shared),
+                       "LDE launch")))
+    return s;
+  if ((s = phases(false, pico_commit::kLde))) return s;
+  // row digests of every height group of every member
+  if ((s = phases(true, pico_commit::kLeaves))) return s;
+  HashBatcher batch;
+  for (size_t i = 0; i < K && !s; i++) {
+    const CommitPlan& plan = *plans[i];
+    for (uint32_t gi = 0; gi < (uint32_t)plan.groups.size(); gi++) {
+      const uint32_t first = plan.groups[gi].first, last = plan.groups[gi].second;
+      if (!batch.fits(plan, first, last)) {
+        if ((s = batch.launch(field, st, ctx->hash_block[field]))) break;
+        shared++;
+      }
+      batch.add(plan, cs[i]->leaves, first, last, 1ull << plan.mats[first].log_N,
+                gi == 0 ? commits[i]->layers : cs[i]->inj[gi]);
+    }
+  }
+  if (!s && !batch.empty()) {
+    s = batch.launch(field, st, ctx->hash_block[field]);
+    shared++;
+  }
+  if (s || (s = phases(false, pico_commit::kLeaves))) return s;
+  // each member's tree and root
+  for (size_t i = 0; i < K; i++) {
+    pico_commit* c = commits[i];
+    c->stats.launches += shared;
+    uint32_t* root = nullptr;
+    if ((s = cuda_status(cudaEventRecord(c->ev[3], st), "event"))) return s;
+    if ((s = enqueue_tree(*plans[i], c->layers, cs[i]->inj, st, &c->stats.launches, &root))) return s;
+    if ((s = cuda_status(cudaEventRecord(c->ev[4], st), "event"))) return s;
+    if ((s = cuda_status(cudaMemcpyAsync(root_host[i], root, 32, cudaMemcpyDeviceToHost, st), "root copy")))
+      return s;
+  }
   return PICO_OK;
 }
 
@@ -1159,7 +1308,7 @@ namespace pico {
 // its per-chunk proving-time table (vm/src/instances/machine/riscv.rs:255-266).
 static std::mutex g_metrics_mu;
 void metrics_record(const char* kind, int field, uint32_t n_mats, uint32_t log_b, uint32_t flags,
-                    const pico_commit_stats& st, double queued_us, double run_us) {
+                    const pico_commit_stats& st, double queued_us, double run_us, uint32_t group) {
   const char* path = getenv("PICO_METRICS_LOG");
   if (!path || !*path) return;
   const double ts = std::chrono::duration<double>(std::chrono::system_clock::now().time_since_epoch()).count();
@@ -1175,7 +1324,8 @@ void metrics_record(const char* kind, int field, uint32_t n_mats, uint32_t log_b
                    (unsigned long long)st.permutations, (unsigned long long)st.launches, st.total_ms, st.h2d_ms,
                    st.lde_ms, st.leaves_ms, st.tree_ms);
   if (queued_us >= 0 && n > 0 && n < (int)sizeof line)
-    n += snprintf(line + n, sizeof line - n, ", \"queued_us\": %.1f, \"run_us\": %.1f", queued_us, run_us);
+    n += snprintf(line + n, sizeof line - n, ", \"queued_us\": %.1f, \"run_us\": %.1f, \"group\": %u", queued_us,
+                  run_us, group);
   if (n <= 0 || n >= (int)sizeof line - 3) return;
   std::lock_guard<std::mutex> g(g_metrics_mu);
   if (FILE* f = fopen(path, "a")) {

@@ -58,6 +58,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
                         CommitPlan& plan);
 
 struct Server;  // serving.h
+constexpr uint32_t kMaxGroup = 16;  // serving: largest group of requests sharing launches
 
 // Stream-ordered device allocation of the library (failure injection for
 // tests included); free with cudaFreeAsync on a stream ordered after st.
@@ -69,6 +70,11 @@ cudaStream_t aux_stream(pico_ctx* ctx);
 TwiddleTables twiddles(pico_ctx* ctx, int field);
 pico_status enqueue_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStream_t st, cudaStream_t cst,
                            pico_commit* c, std::vector<void*>& scratch, uint32_t* root_host);
+// Several extended, batched commits of device inputs of one field on st,
+// sharing their LDE and row-hashing launches (serving admits them together).
+pico_status enqueue_commit_group(pico_ctx* ctx, const std::vector<const CommitPlan*>& plans, cudaStream_t st,
+                                 const std::vector<pico_commit*>& commits, std::vector<void*>& scratch,
+                                 const std::vector<uint32_t*>& root_host);
 void free_commit_buffers(pico_commit* c, cudaStream_t st);
 // Bounds guards of the kernels (GuardRecord): guard_enqueue copies both
 // units' records into the slot's pinned host records on st; after st has
@@ -89,9 +95,10 @@ pico_status guard_enqueue(pico_ctx* ctx, uint32_t slot, cudaStream_t st);
 pico_status guard_verdict(pico_ctx* ctx, uint32_t slot, std::string* msg = nullptr);
 pico_status finish_stats(pico_commit* c);
 // One JSON line per finished commit or served request into the file named by
-// PICO_METRICS_LOG (nothing when unset); queued_us < 0 for synchronous commits.
+// PICO_METRICS_LOG (nothing when unset); queued_us < 0 for synchronous commits;
+// `group`: members of the group a served request was admitted in.
 void metrics_record(const char* kind, int field, uint32_t n_mats, uint32_t log_b, uint32_t flags,
-                    const pico_commit_stats& st, double queued_us, double run_us);
+                    const pico_commit_stats& st, double queued_us, double run_us, uint32_t group = 0);
 
 }  // namespace pico
 
@@ -111,6 +118,7 @@ struct pico_ctx {
   pico::GuardRecord* guard_host = nullptr;  // pinned: 2 records (LDE, hashing) per stream slot
   pico::Server* server = nullptr;
   uint32_t max_inflight = 0;  // serving: requests on the device at once
+  uint32_t max_group = 1;     // serving: requests admitted together into one slot (shared launches)
   // Autotuned choices (pico_gpu_autotune), per field: the LDE's four-step
   // split log2 n1 per height (0 = default) and the row-hashing block size.
   uint8_t lde_split[2][pico::kLdeMaxLogN + 1] = {};

@@ -13,6 +13,11 @@
 //   - each admitted request is enqueued whole on its own stream, so requests
 //     that arrive while others run overlap with them on the device; a host
 //     callback marks completion and returns the scratch budget at once;
+//   - with pico_config.max_group > 1, queued batched requests of device
+//     inputs and the same field join the request just admitted, up to
+//     max_group members and kGroupCells trace cells, each within the budget:
+//     the group runs on one stream with its LDE and row-hashing launches
+//     shared (enqueue_commit_group) and its members finish together;
 //   - LDEs and digest layers stay resident (and budgeted) until the caller
 //     releases the commit handed over by pico_gpu_wait.
 #include <chrono>
@@ -35,15 +40,26 @@ struct pico_request {
   pico_commit* commit = nullptr;
   std::vector<void*> scratch;
   uint32_t root_pinned_idx = 0;
-  uint32_t* root_pinned = nullptr;
+  uint32_t* root_pinned = nullptr;  // 8 words of the slot's pinned root buffers
   uint32_t root[8] = {0};
   int slot = -1;
+  uint32_t group_size = 1;  // members of the group it was admitted in
   Clock::time_point t_submit, t_admit, t_done;
 };
 
 namespace pico {
 
 constexpr int kStarveMs = 200;
+// A group takes no more members once it holds this many trace cells: a
+// commit of 2^28 cells already fills the device, and a larger group would
+// only delay its first member's completion.
+constexpr uint64_t kGroupCells = 1ull << 28;
+
+// Requests admitted together into one stream slot.
+struct Group {
+  std::vector<pico_request*> members;
+  int slot = -1;
+};
 
 struct Server {
   pico_ctx* ctx;
@@ -52,12 +68,16 @@ struct Server {
   std::condition_variable done_cv; // waiters
   std::list<pico_request*> queue;
   std::vector<bool> slot_busy;
-  uint32_t* pinned_roots = nullptr;  // one 8-word slot per stream
+  uint32_t* pinned_roots = nullptr;  // kMaxGroup 8-word roots per stream slot
   bool stop = false;
   std::thread thr;
 
   void run();
   bool admit(pico_request* r);
+  void fill_group(Group* g, Clock::time_point now);
+  bool groupable(const pico_request* r) const {
+    return ctx->max_group > 1 && r->plan.input_device && r->plan.extend && !r->plan.plain;
+  }
 };
 
 static void CUDART_CB on_request_done(void* arg) {
@@ -101,8 +121,105 @@ bool Server::admit(pico_request* r) {
   r->slot = slot;
   r->state = pico_request::RUNNING;
   r->t_admit = Clock::now();
-  r->root_pinned = pinned_roots + 8 * slot;
+  r->root_pinned = pinned_roots + 8 * kMaxGroup * slot;
   return true;
+}
+
+// Caller holds mu.  Moves queued requests that can share the launches of
+// g's first member into g, each claiming its budget; a request that has
+// waited more than kStarveMs and cannot join stops the scan, so that none
+// overtakes it.
+void Server::fill_group(Group* g, Clock::time_point now) {
+  const pico_request* first = g->members[0];
+  if (!groupable(first)) return;
+  uint64_t cells = first->plan.cells;
+  for (auto it = queue.begin(); it != queue.end() && g->members.size() < ctx->max_group;) {
+    pico_request* r = *it;
+    if (groupable(r) && r->plan.field == first->plan.field && cells + r->plan.cells <= kGroupCells &&
+        try_reserve(ctx, r->plan.bytes_resident + r->plan.bytes_scratch)) {
+      r->slot = g->slot;
+      r->state = pico_request::RUNNING;
+      r->t_admit = Clock::now();
+      r->root_pinned = pinned_roots + 8 * (kMaxGroup * g->slot + g->members.size());
+      cells += r->plan.cells;
+      g->members.push_back(r);
+      it = queue.erase(it);
+      continue;
+    }
+    const auto waited = std::chrono::duration_cast<std::chrono::milliseconds>(now - r->t_submit).count();
+    if (waited > kStarveMs) break;
+    ++it;
+  }
+}
+
+// Completion of a group: every member done at once (host memory only, as in
+// on_request_done).
+static void CUDART_CB on_group_done(void* arg) {
+  Group* grp = (Group*)arg;
+  Server* sv = grp->members[0]->ctx->server;
+  for (pico_request* r : grp->members) unreserve(r->ctx, r->plan.bytes_scratch);
+  std::lock_guard<std::mutex> g(sv->mu);
+  const GuardRecord* gr = sv->ctx->guard_host + 2 * grp->slot;
+  const auto done = Clock::now();
+  for (pico_request* r : grp->members) {
+    r->group_size = (uint32_t)grp->members.size();
+    memcpy(r->root, r->root_pinned, 32);
+    memcpy(r->commit->root, r->root_pinned, 32);
+    if (gr[0].count || gr[1].count) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "internal bounds guard: %s kernel skipped an access (tag %llu)",
+               gr[0].count ? "LDE" : "row hashing", gr[0].count ? gr[0].tag : gr[1].tag);
+      r->status = PICO_ERR_CUDA;
+      r->error = buf;
+    }
+    r->t_done = done;
+    r->state = pico_request::DONE;
+  }
+  sv->slot_busy[grp->slot] = false;
+  delete grp;
+  sv->cv.notify_all();
+  sv->done_cv.notify_all();
+}
+
+// Enqueue an admitted group of two or more requests on its slot's stream
+// (without mu held, as launch_request).
+static void launch_group(Server* sv, Group* grp) {
+  pico_ctx* ctx = sv->ctx;
+  cudaStream_t st = ctx->streams[grp->slot];
+  std::vector<const CommitPlan*> plans;
+  std::vector<pico_commit*> commits;
+  std::vector<uint32_t*> roots;
+  for (pico_request* r : grp->members) {
+    r->commit = new pico_commit();
+    plans.push_back(&r->plan);
+    commits.push_back(r->commit);
+    roots.push_back(r->root_pinned);
+  }
+  std::vector<void*> scratch;
+  pico_status s = enqueue_commit_group(ctx, plans, st, commits, scratch, roots);
+  for (void* p : scratch) cudaFreeAsync(p, st);
+  if (s == PICO_OK) s = guard_enqueue(ctx, grp->slot, st);
+  if (s == PICO_OK) s = cuda_status(cudaLaunchHostFunc(st, on_group_done, grp), "completion callback");
+  if (s != PICO_OK) {
+    const std::string msg = pico_gpu_last_error();
+    cudaStreamSynchronize(st);
+    for (pico_request* r : grp->members) free_commit_buffers(r->commit, st);
+    cudaStreamSynchronize(st);
+    for (pico_request* r : grp->members) {
+      delete r->commit;
+      r->commit = nullptr;
+      unreserve(ctx, r->plan.bytes_resident + r->plan.bytes_scratch);
+    }
+    std::lock_guard<std::mutex> g(sv->mu);
+    for (pico_request* r : grp->members) {
+      r->status = s;
+      r->error = msg;
+      r->state = pico_request::FAILED;
+    }
+    sv->slot_busy[grp->slot] = false;
+    delete grp;
+    sv->done_cv.notify_all();
+  }
 }
 
 // Enqueue an admitted request on its stream.  Called without mu held: the
@@ -153,8 +270,17 @@ void Server::run() {
       if (waited > kStarveMs) break;
     }
     if (picked) {
+      Group* grp = new Group();
+      grp->members.push_back(picked);
+      grp->slot = picked->slot;
+      fill_group(grp, now);
       lk.unlock();
-      launch_request(this, picked);
+      if (grp->members.size() == 1) {
+        delete grp;
+        launch_request(this, picked);
+      } else {
+        launch_group(this, grp);
+      }
       lk.lock();
       continue;
     }
@@ -168,7 +294,7 @@ pico_status serving_start(pico_ctx* ctx) {
   auto* sv = new Server();
   sv->ctx = ctx;
   sv->slot_busy.assign(ctx->streams.size(), false);
-  if (cudaMallocHost(&sv->pinned_roots, 32 * ctx->streams.size()) != cudaSuccess) {
+  if (cudaMallocHost(&sv->pinned_roots, 32 * kMaxGroup * ctx->streams.size()) != cudaSuccess) {
     delete sv;
     return cuda_status(cudaGetLastError(), "pinned root buffers");
   }
@@ -293,7 +419,7 @@ extern "C" pico_status pico_gpu_wait(pico_ctx* ctx, pico_request* req, int64_t t
     const uint32_t fl = (req->plan.input_device ? PICO_INPUT_DEVICE : 0u) | (req->plan.plain ? PICO_COMMIT_PLAIN : 0u);
     metrics_record("request", req->plan.field, (uint32_t)req->plan.mats.size(), req->plan.log_b, fl, c->stats,
                    std::chrono::duration<double, std::micro>(req->t_admit - req->t_submit).count(),
-                   std::chrono::duration<double, std::micro>(req->t_done - req->t_admit).count());
+                   std::chrono::duration<double, std::micro>(req->t_done - req->t_admit).count(), req->group_size);
   }
   if (out) {
     *out = c;

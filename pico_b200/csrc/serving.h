@@ -1,5 +1,6 @@
 // Serving path: asynchronous commit requests admitted by free HBM budget and
-// run concurrently on the context's streams (continuous batching).
+// run concurrently on the context's streams, queued ones admitted together
+// as groups that share their launches (continuous batching).
 #pragma once
 #include "runtime.h"
 

@@ -44,12 +44,14 @@ def _log2_exact(n: int) -> int:
 class GpuContext:
     """One device context (pico_gpu_init).  Thread-safe; close() when done."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, n_streams: int = 0, max_inflight: int = 0):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, n_streams: int = 0, max_inflight: int = 0,
+                 max_group: int = 0):
         self.lib = abi.load()
         cfg = abi.Config()
         cfg.hbm_budget_bytes = hbm_budget_bytes
         cfg.n_streams = n_streams
         cfg.max_inflight = max_inflight
+        cfg.max_group = max_group
         h = C.c_void_p()
         abi.check(self.lib.pico_gpu_init(device, C.byref(cfg), C.byref(h)))
         self.handle = h

@@ -9,8 +9,8 @@ oracle.  The benchmarked sizes (full-size roots, FRI at 2^23, LDEs of 2^18 ..
 import numpy as np
 import pytest
 
-from pico_b200 import (CommitServer, MerkleTreeMmcs, PicoError, Poseidon2, Radix2DitParallel, TwoAdicDomain,
-                       TwoAdicFriPcs)
+from pico_b200 import (CommitServer, GpuContext, MerkleTreeMmcs, PicoError, Poseidon2, Radix2DitParallel,
+                       TwoAdicDomain, TwoAdicFriPcs)
 from pico_b200 import fields as F
 
 pytestmark = pytest.mark.gpu
@@ -414,3 +414,50 @@ def test_evaluations_on_domain(gpu, orc, f, log_n, b, extra):
     assert np.array_equal(dev.cpu().numpy().view(np.uint32), got)
     with pytest.raises(PicoError):
         pd.evaluations_on_domain(0, log_n + b + 1)
+
+
+def test_grouped_requests_match_alone(orc, tmp_path, monkeypatch):
+    """Continuous batching: with max_group > 1, device-input requests queued
+    behind a running one are admitted together and share their LDE and
+    row-hashing launches; every root is the one the request gets alone (and
+    the oracle's), across mixed blowups, heights, width-0 matrices and both
+    fields (which never share a group)."""
+    import json
+
+    torch = _torch()
+    log = tmp_path / "metrics.jsonl"
+    monkeypatch.setenv("PICO_METRICS_LOG", str(log))
+    ctx = GpuContext(0, n_streams=2, max_inflight=1, max_group=8)
+    try:
+        server = CommitServer(ctx)
+        rng = np.random.default_rng(17)
+        big = torch.from_numpy(F.random_matrix(0, 18, 64, 77).view(np.int32)).cuda()
+        reqs = [(0, 2, [big], server.submit(0, [big], 2))]  # runs while the others queue
+        for k in range(14):
+            f = 1 if k in (4, 9) else 0
+            b = int(rng.integers(1, 3))
+            shapes = [(int(rng.integers(3, 14)), int(rng.integers(0, 40))) for _ in range(int(rng.integers(1, 7)))]
+            mats = [torch.from_numpy(F.random_matrix(f, lh, w, 2000 * k + i).view(np.int32)).cuda()
+                    for i, (lh, w) in enumerate(shapes)]
+            reqs.append((f, b, mats, server.submit(f, mats, b)))
+        for f, b, mats, r in reqs:
+            root, pd = r.wait(timeout_ms=120000)
+            host = [m.cpu().numpy().view(np.uint32) for m in mats]
+            alone, _ = TwoAdicFriPcs(ctx, f, b).commit(
+                [(TwoAdicDomain(m.shape[0].bit_length() - 1), m) for m in host], keep=False)
+            assert root.tolist() == alone.tolist()
+            if len(host) > 1 or host[0].shape[0] < (1 << 18):
+                want, _, _ = orc.pcs_commit(f, host, [F.lde_shift(f)] * len(host), b)
+                assert root.tolist() == want.tolist()
+            # the prover data of a grouped member reads back like any commit's
+            k = int(np.argmax([m.shape[0] * m.shape[1] for m in host]))
+            if host[k].shape[1]:
+                lde = pd.lde_rows(k, 0, 4)
+                assert lde.shape == (4, host[k].shape[1])
+            pd.release()
+            r.free()
+        assert ctx.memory()[0] == 0
+    finally:
+        ctx.close()
+    groups = [json.loads(l)["group"] for l in log.read_text().splitlines() if json.loads(l)["kind"] == "request"]
+    assert len(groups) == 15 and max(groups) > 1
