@@ -222,6 +222,25 @@ pico_status pico_gpu_noalloc_status(void *stream);
  * shift is ignored. */
 pico_status pico_gpu_mmcs_commit(pico_ctx *ctx, pico_field field, const pico_matrix *mats, uint32_t n_mats,
                                  uint32_t flags, pico_commit **out, uint32_t root[8]);
+/* One shard of TwoAdicFriPcs::commit (prover.rs:102) split by rows over
+ * 2^log_shards devices (no counterpart in the reference, which commits on one
+ * host).  Shard s holds rows [s N / 2^k, (s + 1) N / 2^k) of every committed
+ * LDE (N its height, k = log_shards), i.e. the LDE's coset blocks
+ * s 2^(b-k) .. (s + 1) 2^(b-k) - 1: each shard computes them from the whole
+ * trace, with no exchange between devices, so k <= log_blowup.  It also builds
+ * the Merkle tree over its rows (rows of shorter matrices injected where
+ * their heights meet, as in the full tree); that tree is the full tree's
+ * subtree under the node at depth k, index s, and `root` receives it.
+ * pico_gpu_merkle_top turns the 2^k shard roots into the commitment root.  The
+ * prover data holds the shard's rows (lde_rows and the digest layers count
+ * them from the shard's first row). */
+pico_status pico_gpu_commit_shard(pico_ctx *ctx, pico_field field, const pico_matrix *mats, uint32_t n_mats,
+                                  uint32_t log_blowup, uint32_t log_shards, uint32_t shard, uint32_t flags,
+                                  pico_commit **out, uint32_t root[8]);
+/* The top log_shards levels of a Merkle tree on the host: the 2^log_shards
+ * shard roots (8 words each, in shard order) compressed pairwise up to the
+ * root (MerkleTreeMmcs compression; no device needed). */
+pico_status pico_gpu_merkle_top(pico_field field, const uint32_t *roots, uint32_t log_shards, uint32_t root[8]);
 /* Poseidon2KoalaBear<16> / Poseidon2BabyBear<16> on n states of 16 words, in place. */
 pico_status pico_gpu_poseidon2_permute(pico_ctx *ctx, pico_field field, uint32_t *states, uint64_t n,
                                        uint32_t flags);

@@ -575,7 +575,7 @@ TwiddleTables twiddles(pico_ctx* ctx, int field) {
 // Commit planning
 
 pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t log_b, uint32_t flags, bool extend,
-                        CommitPlan& plan) {
+                        CommitPlan& plan, uint32_t shard_log, uint32_t shard) {
   if (field != PICO_KOALABEAR && field != PICO_BABYBEAR) {
     set_error("unknown field %d", field);
     return PICO_ERR_INVALID_ARG;
@@ -589,9 +589,16 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
     set_error("commit: log_blowup %u is above the supported %u", log_b, kLdeMaxLogBlowup);
     return PICO_ERR_INVALID_ARG;
   }
+  if (shard_log > (extend ? log_b : 0) || (shard_log < 32 && shard >= (1u << shard_log))) {
+    set_error("commit: shard %u of 2^%u: a shard must hold whole coset blocks (at most 2^log_blowup = 2^%u shards)",
+              shard, shard_log, extend ? log_b : 0);
+    return PICO_ERR_INVALID_ARG;
+  }
   plan = CommitPlan{};
   plan.field = field;
   plan.log_b = extend ? log_b : 0;
+  plan.shard_log = shard_log;
+  plan.shard = shard;
   plan.extend = extend;
   plan.input_device = (flags & PICO_INPUT_DEVICE) != 0;
   plan.plain = (flags & PICO_COMMIT_PLAIN) != 0;
@@ -623,7 +630,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
     PlannedMat pm;
     pm.input_idx = i;
     pm.log_n = m.log_height;
-    pm.log_N = m.log_height + plan.log_b;
+    pm.log_N = m.log_height + plan.log_b - shard_log;
     pm.w = (uint32_t)base_w;
     pm.shift = m.shift;
     pm.src = m.values;
@@ -652,7 +659,7 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
       res += cells_out * 4;
       if (!plan.input_device) scr += cells_in * 4;
       if (m.log_n > (uint32_t)kLdeSmallMaxLog) scr += (cells_in + cells_out) * 4;
-      scr += (8192ull << plan.log_b) * 4 + 64;
+      scr += (8192ull << (plan.log_b - shard_log)) * 4 + 64;
     } else if (!plan.input_device) {
       res += cells_in * 4;
     }
@@ -828,7 +835,7 @@ static pico_status setup_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStrea
     chained[gi] = (copy_in || plan.plain) && nonzero_mats(plan, gi) >= 2;
     if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
   }
-  const uint32_t nb = 1u << plan.log_b;
+  const uint32_t nb = 1u << (plan.log_b - plan.shard_log);  // coset blocks per LDE
   std::vector<uint64_t> in_bytes(n, 0), ix_in(n, kNone), ix_out(n, kNone), ix_t1(n, kNone), ix_t2(n, kNone);
   for (uint32_t k = 0; k < n; k++) {
     const PlannedMat& m = plan.mats[k];
@@ -940,6 +947,8 @@ static pico_status setup_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStrea
       L.in = dev_in[k];
       L.log_n = m.log_n;
       L.log_b = plan.log_b;
+      L.shard_log = plan.shard_log;
+      L.shard = plan.shard;
       L.w = m.w;
       L.shift = m.shift % (field == 0 ? KoalaBear::P : BabyBear::P);
       L.pw = pw + (uint64_t)k * nb * kPwWords;
@@ -1340,7 +1349,7 @@ void metrics_record(const char* kind, int field, uint32_t n_mats, uint32_t log_b
 
 static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_matrix* mats, uint32_t n_mats,
                                  uint32_t log_blowup, uint32_t flags, pico_commit** out, uint32_t root[8],
-                                 bool extend) {
+                                 bool extend, uint32_t shard_log = 0, uint32_t shard = 0) {
   if (!ctx || !root) {
     set_error("commit: null context or root");
     return PICO_ERR_INVALID_ARG;
@@ -1348,7 +1357,7 @@ static pico_status commit_common(pico_ctx* ctx, pico_field field, const pico_mat
   if (out) *out = nullptr;
   pico_status s;
   CommitPlan plan;
-  if ((s = plan_commit(field, mats, n_mats, log_blowup, flags, extend, plan))) return s;
+  if ((s = plan_commit(field, mats, n_mats, log_blowup, flags, extend, plan, shard_log, shard))) return s;
   const uint64_t need = plan.bytes_resident + plan.bytes_scratch;
   if (!try_reserve(ctx, need)) {
     set_error("commit: needs %llu bytes, HBM budget has %llu of %llu reserved", (unsigned long long)need,
@@ -1400,6 +1409,33 @@ extern "C" pico_status pico_gpu_commit(pico_ctx* ctx, pico_field field, const pi
 extern "C" pico_status pico_gpu_mmcs_commit(pico_ctx* ctx, pico_field field, const pico_matrix* mats,
                                             uint32_t n_mats, uint32_t flags, pico_commit** out, uint32_t root[8]) {
   return commit_common(ctx, field, mats, n_mats, 0, flags, out, root, false);
+}
+
+extern "C" pico_status pico_gpu_commit_shard(pico_ctx* ctx, pico_field field, const pico_matrix* mats,
+                                             uint32_t n_mats, uint32_t log_blowup, uint32_t log_shards,
+                                             uint32_t shard, uint32_t flags, pico_commit** out, uint32_t root[8]) {
+  return commit_common(ctx, field, mats, n_mats, log_blowup, flags, out, root, true, log_shards, shard);
+}
+
+// The tree's top levels over the shard roots: TruncatedPermutation
+// compressions, left || right -> the first 8 words of the permuted state.
+extern "C" pico_status pico_gpu_merkle_top(pico_field field, const uint32_t* roots, uint32_t log_shards,
+                                           uint32_t root[8]) {
+  if ((field != PICO_KOALABEAR && field != PICO_BABYBEAR) || !roots || !root || log_shards > 20) {
+    set_error("merkle_top: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  std::vector<uint32_t> level(roots, roots + (8ull << log_shards));
+  for (uint32_t l = log_shards; l > 0; l--) {
+    for (uint64_t i = 0; i < (1ull << (l - 1)); i++) {
+      uint32_t s[16];
+      memcpy(s, &level[16 * i], 64);
+      host_permute(field, s);
+      memcpy(&level[8 * i], s, 32);
+    }
+  }
+  memcpy(root, level.data(), 32);
+  return PICO_OK;
 }
 
 extern "C" pico_status pico_gpu_commit_stats(const pico_commit* c, pico_commit_stats* out) {

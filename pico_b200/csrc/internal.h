@@ -135,16 +135,31 @@ cudaError_t launch_challenger_observe(int field, DevChallenger* ch, const uint32
                                       cudaStream_t st);
 
 // --- LDE kernels (ntt_kernels.cu) ----------------------------------------
+// The committed LDE of one matrix is 2^b coset blocks of n rows (block cb =
+// the evaluations on the coset shift * w_N^rev_b(cb) * H_n, bit-reversed).
+// With shard_log = k > 0 (k <= b), only the 2^(b-k) blocks of shard s are
+// computed, cb in [s * 2^(b-k), (s+1) * 2^(b-k)): rows [s N / 2^k, (s+1) N / 2^k)
+// of the committed LDE; out, t2 and pw then hold those blocks only.
 struct LdeMat {
   const uint32_t* in;  // n x w evaluations
-  uint32_t* out;       // N x w, bit-reversed rows
+  uint32_t* out;       // (n << (b - k)) x w, bit-reversed rows
   uint32_t* t1;        // n x w scratch (three-pass form only)
-  uint32_t* t2;        // N x w scratch (three-pass form only)
-  uint32_t* pw;        // 2^b tables of 8192 words: g_cb^i / n, two-level
+  uint32_t* t2;        // (n << (b - k)) x w scratch (three-pass form only)
+  uint32_t* pw;        // 2^(b-k) tables of 8192 words: g_cb^i / n, two-level
   uint32_t log_n, log_b, w;
   uint32_t log_n1, log_n2; // three-pass split n = n1 * n2 (0 for the one-pass form)
   uint32_t shift;          // coset shift, Monty form
+  uint32_t shard_log, shard;  // k and s above (0, 0: every block)
 };
+// Coset blocks an LDE computes (log2) and the first one.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline uint32_t lde_log_c(const LdeMat& m) { return m.log_b - m.shard_log; }
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline uint32_t lde_cb0(const LdeMat& m) { return m.shard << lde_log_c(m); }
 constexpr int kLdeSmallMaxLog = 11;  // one-pass form handles n <= 2^11
 constexpr uint32_t kLdeMaxLogN = 24;  // coset power tables cover exponents below 2^24
 constexpr int kLdeBatch = 32;        // matrices per launch (descriptors travel as kernel parameters)

@@ -6,6 +6,9 @@
 // g_cb = shift * w_N^rev_b(cb) -> NTT_n(d) in bit-reversed order.  Output row
 // cb*n + j then holds f(shift * w_N^rev_N(cb*n + j)), i.e. committed row i is
 // f(shift * w_N^rev(i)) (vm/src/compiler/recursion/circuit/fri.rs:155-171).
+// A shard (LdeMat.shard_log > 0) computes a contiguous range of the blocks:
+// every loop over cb below runs over the shard's 2^(b-k) blocks, which sit
+// at the start of out, t2 and pw; only the power tables need the global cb.
 //
 // Tiles.  A CTA of 512 threads stages a tile of L = 2^l positions x LW lines
 // in shared memory (L * LW = 2^13 words, 32 KiB plus padding, for l >= 4); a line is one
@@ -138,7 +141,7 @@ PICO_HD uint32_t lde_tiles(const LdeMat& m, int pass) {
   if ((pass == kPassSmall) != (m.log_n1 == 0)) return 0u;
   const PassGeom g = pass_geom(m, pass);
   const uint32_t t = g.groups * g.n_ct;
-  return pass == kPassC ? t << m.log_b : t;
+  return pass == kPassC ? t << lde_log_c(m) : t;
 }
 
 PICO_HD uint32_t pass_log_L(const LdeMat& m, int pass) {
@@ -583,7 +586,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassSmall, blockIdx.x, local);
   s_in = GuardRange{M.in, M.in + (((uint64_t)M.w << M.log_n))};
-  s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + lde_log_c(M))))};
   s_smem_words = tile_words_l(LOG_L);
   const TileCtx T = tile_ctx(pass_geom(M, kPassSmall), local, M.w);
   const uint32_t w = M.w;
@@ -591,11 +594,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
     // height 1: every LDE row equals the input row (the scale g^0 / 1 is 1)
     uint32_t col, sub;
     if (line_at(T, threadIdx.x, col, sub))
-      for (uint32_t cb = 0; cb < (1u << M.log_b); cb++) {
+      for (uint32_t cb = 0; cb < (1u << lde_log_c(M)); cb++) {
         const uint32_t* pi = M.in + col;
         uint32_t* po = M.out + (uint64_t)cb * w + col;
         if (pi < M.in || pi >= M.in + w) { guard_trip(kGuardLoad, col, w); continue; }
-        if (po < M.out || po >= M.out + ((uint64_t)w << M.log_b)) { guard_trip(kGuardStore, (uint64_t)cb * w + col, (uint64_t)w << M.log_b); continue; }
+        if (po < M.out || po >= M.out + ((uint64_t)w << lde_log_c(M))) { guard_trip(kGuardStore, (uint64_t)cb * w + col, (uint64_t)w << lde_log_c(M)); continue; }
         *po = __ldg(pi);
       }
   } else {
@@ -614,7 +617,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lde_small(const __grid_constant
     constexpr int RF = LOG_L < 4 ? LOG_L : 4;
     constexpr int RL = fwd_last_r<LOG_L>();
     const uint32_t nm = n_monty<F>(LOG_L);
-    for (uint32_t cb = 0; cb < (1u << M.log_b); cb++) {
+    for (uint32_t cb = 0; cb < (1u << lde_log_c(M)); cb++) {
       const uint32_t* pt = pw_table(M, cb);
       // coefficient i scales by g^i / n: {g^o / n, g^stride} along a set
       // (table entries carry the 1/n, so the step is multiplied back by n)
@@ -683,7 +686,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_b(const __grid_constant__ L
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassB, blockIdx.x, local);
   s_in = GuardRange{M.t1, M.t1 + (((uint64_t)M.w << M.log_n))};
-  s_out = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_out = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + lde_log_c(M))))};
   s_smem_words = tile_words_l(LOG_L);
   const TileCtx T = tile_ctx(pass_geom(M, kPassB), local, M.w);
   const uint32_t w = M.w, log_n1 = M.log_n1;
@@ -702,7 +705,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_b(const __grid_constant__ L
   uint32_t coef[16], line, q;
   inverse_to_regs<F, LOG_L>(buf, twi, line_base, (uint64_t)w, twist, coef, line, q);
   const uint32_t nm = n_monty<F>(M.log_n);
-  for (uint32_t cb = 0; cb < (1u << M.log_b); cb++) {
+  for (uint32_t cb = 0; cb < (1u << lde_log_c(M)); cb++) {
     const uint32_t* pt = pw_table(M, cb);
     // coefficient i = k1 + n1 * p scales by g^i / n: {g^(k1 + n1 o) / n, g^(n1 stride)}
     const uint32_t step = Fp<F>::mul(pw_at<F>(pt, 1u << (LOG_L - 4 + log_n1)), nm);
@@ -738,8 +741,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
   extern __shared__ uint32_t smem[];
   uint32_t local;
   const LdeMat& M = find_tile(batch, kPassC, blockIdx.x, local);
-  s_in = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + M.log_b)))};
-  s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + M.log_b)))};
+  s_in = GuardRange{M.t2, M.t2 + (((uint64_t)M.w << (M.log_n + lde_log_c(M))))};
+  s_out = GuardRange{M.out, M.out + (((uint64_t)M.w << (M.log_n + lde_log_c(M))))};
   s_smem_words = tile_words_l(LOG_L);
   const PassGeom g = pass_geom(M, kPassC);
   const TileCtx T = tile_ctx(g, local, M.w);
@@ -773,17 +776,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_lde_c(const __grid_constant__ L
 }
 
 // ---------------------------------------------------------------------------
-// Power tables of matrix blockIdx.y: for coset cb, entries [0, 4096) hold
-// g^e / n and [4096, 8192) hold g^(4096 e), g = shift * w_N^rev_b(cb).
+// Power tables of matrix blockIdx.y: for the cb-th coset block it computes
+// (global block cb0 + cb), entries [0, 4096) hold g^e / n and [4096, 8192)
+// hold g^(4096 e), g = shift * w_N^rev_b(cb0 + cb).
 template <class F>
 __global__ void k_pow_tables(const __grid_constant__ LdeBatch batch, const __grid_constant__ TwiddleTables tw) {
   using B = Fp<F>;
   const LdeMat& M = batch.m[blockIdx.y];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (kPwWords << M.log_b)) return;
+  if (i >= (kPwWords << lde_log_c(M))) return;
   const uint32_t cb = i / kPwWords, e = i % kPwWords;
   const uint32_t log_N = M.log_n + M.log_b;
-  const uint32_t g = B::mul(M.shift, omega<F>(tw, log_N, bitrev32(cb, M.log_b), false));
+  const uint32_t g = B::mul(M.shift, omega<F>(tw, log_N, bitrev32(lde_cb0(M) + cb, M.log_b), false));
   uint32_t v;
   if (e < 4096u) {
     // 1/2^log_n = p - (p - 1) / 2^log_n (canonical), since 2^log_n * ((p-1)/2^log_n) = -1
@@ -792,7 +796,7 @@ __global__ void k_pow_tables(const __grid_constant__ LdeBatch batch, const __gri
   } else {
     v = B::pow(g, (uint64_t)(e - 4096u) << 12);
   }
-  if (i >= (kPwWords << M.log_b)) { guard_trip(kGuardStore, i, kPwWords << M.log_b); return; }
+  if (i >= (kPwWords << lde_log_c(M))) { guard_trip(kGuardStore, i, kPwWords << lde_log_c(M)); return; }
   M.pw[i] = v;
 }
 
@@ -892,7 +896,7 @@ static cudaError_t launch_lde_t(const LdeMat* mats, uint32_t n_mats, TwiddleTabl
     uint32_t max_b = 0;
     for (uint32_t k = 0; k < all.n; k++) {
       all.m[k] = mats[base + k];
-      max_b = std::max(max_b, all.m[k].log_b);
+      max_b = std::max(max_b, lde_log_c(all.m[k]));
     }
     dim3 pgrid((kPwWords << max_b) / 256, all.n);
     k_pow_tables<F><<<pgrid, 256, 0, st>>>(all, tw);

@@ -46,6 +46,10 @@ struct CommitPlan {
   // height groups in commit order: [begin, end) into mats
   std::vector<std::pair<uint32_t, uint32_t>> groups;
   uint32_t log_max = 0;
+  // One shard of a commit split by rows over 2^shard_log devices: every LDE
+  // computes only its rows [shard N / 2^k, (shard + 1) N / 2^k) (k <= log_b),
+  // and log_N / log_max count the shard's rows.
+  uint32_t shard_log = 0, shard = 0;
   uint64_t bytes_resident = 0;   // LDEs + digest layers
   uint64_t bytes_scratch = 0;    // input copies, NTT scratch, tables
   uint64_t cells = 0;            // sum of trace cells
@@ -55,7 +59,7 @@ struct CommitPlan {
 };
 
 pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t log_b, uint32_t flags, bool extend,
-                        CommitPlan& plan);
+                        CommitPlan& plan, uint32_t shard_log = 0, uint32_t shard = 0);
 
 struct Server;  // serving.h
 constexpr uint32_t kMaxGroup = 16;  // serving: largest group of requests sharing launches

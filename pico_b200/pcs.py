@@ -385,6 +385,20 @@ class TwoAdicFriPcs:
         pd = ProverData(self.ctx, h, root, n, self.field) if keep else None
         return root, pd
 
+    def commit_shard(self, domains_and_traces, log_shards: int, shard: int, keep: bool = True):
+        """Shard `shard` of 2^log_shards of the same commit split by rows
+        (pico_gpu_commit_shard): its rows of every committed LDE and the root
+        of their subtree.  log_shards <= log_blowup."""
+        n = len(domains_and_traces)
+        mats, flags = self._descriptors(domains_and_traces, False)
+        root = np.zeros(8, dtype=np.uint32)
+        h = C.c_void_p()
+        abi.check(self.ctx.lib.pico_gpu_commit_shard(
+            self.ctx.handle, self.field, mats, n, self.log_blowup, log_shards, shard, flags,
+            C.byref(h) if keep else None, root.ctypes.data_as(C.POINTER(C.c_uint32))))
+        pd = ProverData(self.ctx, h, root, n, self.field) if keep else None
+        return root, pd
+
     def get_evaluations_on_domain(self, prover_data: ProverData, idx: int):
         """The committed LDE of matrix idx (bit-reversed rows, as stored)."""
         return prover_data.lde(idx)
@@ -525,3 +539,14 @@ class CommitServer:
         h = C.c_void_p()
         abi.check(self.ctx.lib.pico_gpu_submit_commit(self.ctx.handle, f, mats, n, log_blowup, flags, C.byref(h)))
         return CommitRequest(self, h, n, f)
+
+
+def merkle_top(field, shard_roots) -> np.ndarray:
+    """Root of a Merkle tree from its 2^k subtree roots at depth k, in order
+    (pico_gpu_merkle_top; host only)."""
+    roots = np.ascontiguousarray(np.asarray(shard_roots, dtype=np.uint32).reshape(-1, 8))
+    k = _log2_exact(roots.shape[0])
+    out = np.zeros(8, dtype=np.uint32)
+    abi.check(abi.load().pico_gpu_merkle_top(F.field_id(field), roots.ctypes.data_as(C.POINTER(C.c_uint32)), k,
+                                             out.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return out

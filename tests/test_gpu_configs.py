@@ -20,7 +20,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from pico_b200 import Radix2DitParallel, TwoAdicDomain, TwoAdicFriPcs
+from pico_b200 import PicoError, Radix2DitParallel, TwoAdicDomain, TwoAdicFriPcs
 from pico_b200 import fields as F
 
 pytestmark = pytest.mark.gpu
@@ -133,3 +133,26 @@ def test_wide_lde_2_20_every_split(gpu, orc, f):
             assert (got == want).all(), n1
     finally:
         gpu.lde_split(f, logn, default)
+
+
+@pytest.mark.parametrize("f,logn,b", [(0, 23, 1), (1, 24, 2)])
+def test_lde_at_maximum_height(gpu, orc, f, logn, b):
+    """The tallest LDEs each field allows: KoalaBear 2^23 rows at blowup 2
+    (2^24 = its two-adicity), BabyBear 2^24 rows (the library's limit) at
+    blowup 4, one column, at the default split and at the most unbalanced
+    accepted one."""
+    m = orc.random_matrix(f, logn, 1, 7400 + f)
+    shift = F.lde_shift(f)
+    want = orc.coset_lde(f, m, b, shift)
+    default = gpu.lde_split(f, logn)
+    dft = Radix2DitParallel(gpu, f)
+    try:
+        for n1 in (default, valid_splits(logn)[0]):
+            gpu.lde_split(f, logn, n1)
+            got = dft.coset_lde_batch_bitrev(m, b, shift)
+            assert (got == want).all(), n1
+    finally:
+        gpu.lde_split(f, logn, default)
+    if f == 0:  # one more doubling passes the two-adicity
+        with pytest.raises(PicoError):
+            dft.coset_lde_batch_bitrev(m, b + 1, shift)

@@ -461,3 +461,53 @@ def test_grouped_requests_match_alone(orc, tmp_path, monkeypatch):
         ctx.close()
     groups = [json.loads(l)["group"] for l in log.read_text().splitlines() if json.loads(l)["kind"] == "request"]
     assert len(groups) == 15 and max(groups) > 1
+
+
+@pytest.mark.parametrize("f,b,k", [(0, 1, 1), (1, 2, 2), (0, 2, 1), (1, 1, 0)])
+def test_row_split_commit(gpu, orc, f, b, k):
+    """pico_gpu_commit_shard: shard s of 2^k holds rows [s N / 2^k, (s+1) N / 2^k)
+    of every committed LDE (both LDE forms, heights 2^0 .. 2^14) and its
+    root is the full tree's node s at depth k; merkle_top over the shard
+    roots is the commitment root.  More shards than coset blocks is refused."""
+    from pico_b200.pcs import merkle_top
+
+    shapes = [(14, 3), (12, 2), (9, 5), (6, 1), (0, 2)]
+    mats = [F.random_matrix(f, lh, w, 9100 + 17 * i + f) for i, (lh, w) in enumerate(shapes)]
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    doms = [pcs.natural_domain_for_degree(m.shape[0]) for m in mats]
+    full, pd_full = pcs.commit(list(zip(doms, mats)))
+    want, ldes, layers = orc.pcs_commit(f, mats, [F.lde_shift(f)] * len(mats), b, want_ldes=True, want_layers=True)
+    assert full.tolist() == want.tolist()
+    depth_k = layers[len(layers) - (2 << k) + 1: len(layers) - (1 << k) + 1]
+    subs = []
+    for s in range(1 << k):
+        sub, pd = pcs.commit_shard(list(zip(doms, mats)), k, s)
+        assert sub.tolist() == depth_k[s].tolist(), s
+        for i, l in enumerate(ldes):
+            rows = l.shape[0] >> k
+            assert pd.lde_shape(i) == (rows, l.shape[1])
+            if l.shape[1]:
+                assert np.array_equal(pd.lde_rows(i), l[s * rows:(s + 1) * rows]), (s, i)
+        pd.release()
+        subs.append(sub)
+    assert merkle_top(f, np.stack(subs)).tolist() == want.tolist()
+    pd_full.release()
+    with pytest.raises(PicoError):
+        pcs.commit_shard(list(zip(doms, mats)), b + 1, 0, keep=False)
+    assert gpu.memory()[0] == 0
+
+
+def test_row_split_commit_device_inputs_at_2_20(gpu, orc):
+    """Two shards of a 2^20-row commit from device inputs (three-pass LDE at
+    the autotuner's default split): shard roots and the combined root."""
+    from pico_b200.pcs import merkle_top
+
+    torch = _torch()
+    f, b = 0, 1
+    host = [F.random_matrix(f, 20, 4, 9200), F.random_matrix(f, 17, 3, 9201)]
+    dev = [torch.from_numpy(m.view(np.int32)).cuda() for m in host]
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    doms = [pcs.natural_domain_for_degree(m.shape[0]) for m in host]
+    want, _, _ = orc.pcs_commit(f, host, [F.lde_shift(f)] * 2, b)
+    subs = [pcs.commit_shard(list(zip(doms, dev)), 1, s, keep=False)[0] for s in range(2)]
+    assert merkle_top(f, np.stack(subs)).tolist() == want.tolist()
