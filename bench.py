@@ -828,6 +828,11 @@ def run_quotient(args):
     cpu_s = time.perf_counter() - t
     ctx.close()
     points = Q
+    # algorithmic bytes: every point's main and permutation row read once (the
+    # next-row reads are other points' rows) and its EF4 quotient written
+    q_bytes = Q * 4 * (main_w + 4 + 4)
+    hbm_peak, hbm_kind = peaks()
+    q_ach = q_bytes / (ms / 1e3) / 1e9
     return {
         "metric": "quotient-domain points/sec (compute_quotient_values of one chip, resident LDEs)",
         "value": points / (ms / 1e3), "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -837,6 +842,12 @@ def run_quotient(args):
                    "main_width": main_w, "perm_width": 1, "program_ops": int(prog.shape[0])},
         "parity": {"matches_oracle": match, "points": points},
         "clocks": clocks,
+        "gpu_launches": args.steps,
+        "roofline": {"kernel": "k_quotient", "bound": "hbm", "achieved": q_ach, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": q_ach / hbm_peak, "traffic": None, "algorithmic_bytes": q_bytes,
+                     "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback",
+                     "note": "the kernel interprets the constraint program per point, so its instruction stream, not "
+                             "HBM, bounds it; the fraction shows how far the trace reads are from limiting it"},
         "cpu_baseline": {"value": (2 << small) / cpu_s, "unit": "points/s", "cores": orc.num_threads(),
                          "kind": "port", "cpu_model": cpu_model(),
                          "sample": f"the same program on a 2^{small}-row trace ({2 << small} points), one run"},
@@ -990,7 +1001,8 @@ def run_serving(args):
             forms.insert(1, ("grouped", False, server_g))
         for name, plain, srv in forms:
             s_, lat, queued = served(plain, arrivals, srv)
-            row[name] = {"cells_per_s": total_cells / s_, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+            row[name] = {"cells_per_s": total_cells / s_, "p50_ms": pct(lat, 50), "p90_ms": pct(lat, 90),
+                         "p99_ms": pct(lat, 99), "max_ms": pct(lat, 100),
                          "mean_queue_ms": float(np.mean(queued) * 1e3)}
         sweep.append(row)
     ctx_g.close()

@@ -18,6 +18,7 @@
 // three inverses share one Fermat inversion per point.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -29,9 +30,8 @@
 namespace pico {
 
 constexpr int kQThreads = 128;
-constexpr uint32_t kQBaseRegs = 64;
+constexpr uint32_t kQBaseRegs = 64;  // register file limits of a program
 constexpr uint32_t kQExtRegs = 16;
-constexpr size_t kQSmemBytes = (kQBaseRegs + 4 * kQExtRegs) * kQThreads * 4;  // 64 KiB
 
 struct QuotientArgs {
   const uint32_t* main;
@@ -44,6 +44,7 @@ struct QuotientArgs {
   const uint32_t* chal;     // permutation challenges, 4 words each
   const uint32_t* consts;   // regional sum (4), global sum (14), alpha (4)
   uint32_t log_trace, log_qd;
+  uint32_t n_base;          // base registers the program uses; the extension registers follow them
   uint32_t* out;            // Q x 4
 };
 
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(kQThreads) k_quotient(const __grid_constant__ 
   using E = Ef<F>;
   extern __shared__ uint32_t qsm[];
   uint32_t* rb = qsm + threadIdx.x;                               // base register r at rb[r * kQThreads]
-  uint32_t* re = qsm + kQBaseRegs * kQThreads + threadIdx.x;      // ext register r, coeff j at re[(4r+j) * kQThreads]
+  uint32_t* re = qsm + A.n_base * kQThreads + threadIdx.x;        // ext register r, coeff j at re[(4r+j) * kQThreads]
   const uint32_t log_q = A.log_trace + A.log_qd;
   const uint64_t Q = 1ull << log_q;
   const uint64_t i = (uint64_t)blockIdx.x * kQThreads + threadIdx.x;
@@ -214,7 +215,10 @@ extern "C" pico_status pico_gpu_quotient_values(pico_ctx* ctx, pico_trace_ref pr
     set_error("quotient_values: the permutation trace has %u words per row, not whole extension elements", we);
     return PICO_ERR_INVALID_ARG;
   }
-  // the program: every register, column and table index in range
+  // the program: every register, column and table index in range; the
+  // register files are sized to the highest register it names, so a small
+  // program leaves shared memory for more resident CTAs
+  uint32_t n_base = 1, n_ext = 1;
   for (uint32_t k = 0; k < n_ops; k++) {
     const pico_constraint_op& o = program[k];
     bool ok;
@@ -242,7 +246,23 @@ extern "C" pico_status pico_gpu_quotient_values(pico_ctx* ctx, pico_trace_ref pr
                 o.dst, o.a, o.b);
       return PICO_ERR_INVALID_ARG;
     }
+    // registers named (in range, checked above): which operands are base or extension registers
+    auto base = [&](uint32_t r) { n_base = std::max(n_base, r + 1); };
+    auto ext = [&](uint32_t r) { n_ext = std::max(n_ext, r + 1); };
+    switch (o.op) {
+      case PICO_Q_MAIN: case PICO_Q_PREP: case PICO_Q_CONST: case PICO_Q_PUBLIC: case PICO_Q_FIRST:
+      case PICO_Q_LAST: case PICO_Q_TRANSITION: case PICO_Q_GLOBAL: base(o.dst); break;
+      case PICO_Q_ADD: case PICO_Q_SUB: case PICO_Q_MUL: base(o.dst); base(o.a); base(o.b); break;
+      case PICO_Q_PERM: case PICO_Q_CHALLENGE: case PICO_Q_REGIONAL: ext(o.dst); break;
+      case PICO_Q_EADD: case PICO_Q_ESUB: case PICO_Q_EMUL: ext(o.dst); ext(o.a); ext(o.b); break;
+      case PICO_Q_EMB: ext(o.dst); base(o.a); break;
+      case PICO_Q_EMULB: ext(o.dst); ext(o.a); base(o.b); break;
+      case PICO_Q_ASSERT: base(o.a); break;
+      case PICO_Q_EASSERT: ext(o.a); break;
+      default: break;
+    }
   }
+  const size_t smem = (size_t)(n_base + 4 * n_ext) * kQThreads * 4;  // at most 64 KiB
   const uint64_t Q = 1ull << log_q;
   const bool out_dev = flags & PICO_OUTPUT_DEVICE;
   // one device block: program, public values, challenges, constants, then the output if on the host
@@ -284,17 +304,18 @@ extern "C" pico_status pico_gpu_quotient_values(pico_ctx* ctx, pico_trace_ref pr
   A.consts = blk + w_ops + w_pub + w_chal;
   A.log_trace = log_trace_height;
   A.log_qd = log_quotient_degree;
+  A.n_base = n_base;
   A.out = out_dev ? out : blk + off_out;
   const TwiddleTables tw = twiddles(ctx, field);
   const unsigned grid = (unsigned)((Q + kQThreads - 1) / kQThreads);
   if (!s) {
     cudaError_t e;
     if (field == PICO_KOALABEAR) {
-      e = cudaFuncSetAttribute(k_quotient<KoalaBear>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmemBytes);
-      if (!e) k_quotient<KoalaBear><<<grid, kQThreads, kQSmemBytes, st>>>(A, tw);
+      e = cudaFuncSetAttribute(k_quotient<KoalaBear>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (!e) k_quotient<KoalaBear><<<grid, kQThreads, smem, st>>>(A, tw);
     } else {
-      e = cudaFuncSetAttribute(k_quotient<BabyBear>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmemBytes);
-      if (!e) k_quotient<BabyBear><<<grid, kQThreads, kQSmemBytes, st>>>(A, tw);
+      e = cudaFuncSetAttribute(k_quotient<BabyBear>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (!e) k_quotient<BabyBear><<<grid, kQThreads, smem, st>>>(A, tw);
     }
     s = cuda_status(e ? e : cudaGetLastError(), "quotient kernel");
   }
