@@ -102,6 +102,13 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout: float = 5.0):
+        """Block until nvidia-smi has printed its first sample, so that a timed
+        region shorter than its start-up still has samples around it."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.005)
+
     def stop(self):
         if self.proc:
             self.proc.terminate()
@@ -315,6 +322,7 @@ def run_gpu(args, rank, world, local):
         torch.cuda.synchronize()
         sampler = ClockSampler(local)
         sampler.start()
+        sampler.wait_first()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -612,6 +620,7 @@ def run_open(args, rank, world, local):
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
+    sampler.wait_first()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     outs = [step() for _ in range(args.steps)]
@@ -707,10 +716,15 @@ def run_fri(args):
     torch.cuda.synchronize()
     pcs = TwoAdicFriPcs(ctx, f, b)
     out = {}
+    clocks = None
     for name, lf in (("final_1", 0), ("final_16", 4)):
         for _ in range(args.warmup):
             pcs.fri_commit_phase(cw, log_final_len=lf)
         torch.cuda.synchronize()
+        if name == "final_1":
+            sampler = ClockSampler(0)
+            sampler.start()
+            sampler.wait_first()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(args.steps):
@@ -718,6 +732,8 @@ def run_fri(args):
         torch.cuda.synchronize()
         e1.record()
         e1.synchronize()
+        if name == "final_1":
+            clocks = sampler.stop()
         ms = e0.elapsed_time(e1) / args.steps
         out[name] = {"ms": ms, "rounds": res.rounds, "elements_per_s": (1 << (log_trace + b)) / (ms / 1e3)}
         gold = json.loads(GOLDEN_ROOTS.read_text()).get("fri-kb-2^23") if GOLDEN_ROOTS.exists() else None
@@ -725,13 +741,55 @@ def run_fri(args):
             g = gold[name]
             out[name]["matches_oracle"] = (res.roots.tolist() == g["roots"] and res.betas.tolist() == g["betas"]
                                            and res.final_poly.tolist() == g["final"])
+    # end to end: the codeword from pinned host memory, roots, betas and the
+    # final polynomial back to the host, per call
+    n_el = 1 << (log_trace + b)
+    cw_host = torch.empty((n_el, 4), dtype=torch.int32, pin_memory=True)
+    cw_host.copy_(cw)
+    cw_np = cw_host.numpy().view(np.uint32)
+    for _ in range(args.warmup):
+        pcs.fri_commit_phase(cw_np)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        pcs.fri_commit_phase(cw_np)
+    e2e_s = (time.perf_counter() - t) / args.steps
+    rounds = out["final_1"]["rounds"]
     ctx.close()
+    # Poseidon2 work of a phase: per round, one permutation per leaf (two EF4
+    # elements = eight words) and one per internal node of the round's tree
+    perms = sum((1 << (log_trace + b - 1 - r)) + (1 << (log_trace + b - 1 - r)) - 1 for r in range(rounds))
+    imad_peak = 148 * IMAD_PER_SM_CLK * ((clocks or {}).get("sm_mhz") or 1965.0) / 1e6
+    imad_ach = perms * PERM_MODMULS[f] * IMAD_PER_MODMUL / (out["final_1"]["ms"] / 1e3) / 1e12
+    # CPU: the oracle's commit phase of a 2^17-element codeword of the same kind
+    from oracle import cpu as orc
+
+    small = 19
+    cw_small = orc.coset_lde(f, orc.random_matrix(f, small, 4, 4001), b, F.lde_shift(f))
+    runs = []
+    for _ in range(3):
+        t = time.perf_counter()
+        orc.fri_commit_phase(f, cw_small, b, 0)
+        runs.append(time.perf_counter() - t)
+    cpu_s = float(np.median(runs))
     return {
         "metric": "FRI commit-phase codeword elements/sec (EF4, arity 2, Poseidon2 layer commits)",
         "value": out["final_1"]["elements_per_s"], "unit": "elements/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": out["final_1"]["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (KoalaBear EF4)", "data": "synthetic: random degree < 2^22 EF4 polynomial",
-        "config": {"workload": "fri-kb-2^23", "log_n": log_trace + b, "log_blowup": b}, "modes": out,
+        "config": {"workload": "fri-kb-2^23", "log_n": log_trace + b, "log_blowup": b,
+                   "l2": "codeword 128 MiB and its layers exceed L2 (126 MB); no flush"},
+        "modes": out,
+        "clocks": clocks,
+        "e2e": {"value": n_el / e2e_s, "unit": "elements/s", "ms_per_step": e2e_s * 1e3,
+                "h2d_bytes_per_step": n_el * 16, "d2h_bytes_per_step": rounds * 48 + 16},
+        "roofline": {"kernel": "the phase's Poseidon2 kernels (k_fri_fold_hash, k_compress, k_subtree_quad, "
+                               "k_tree_top)", "bound": "imad", "achieved": imad_ach, "peak": imad_peak,
+                     "unit": "Tops/s", "frac": imad_ach / imad_peak, "traffic": None, "permutations": perms,
+                     "note": "survey model: 4 IMAD x modmuls per permutation; the phase is bound by chains of "
+                             "dependent permutations (each round's leaves need the previous round's beta)"},
+        "cpu_baseline": {"value": (1 << (small + b)) / cpu_s, "unit": "elements/s", "cores": orc.num_threads(),
+                         "kind": "port", "cpu_model": cpu_model(),
+                         "sample": f"the oracle's commit phase of a 2^{small + b}-element codeword, median of 3"},
     }
 
 
@@ -801,6 +859,7 @@ def run_quotient(args):
     torch.cuda.synchronize()
     sampler = ClockSampler(0)
     sampler.start()
+    sampler.wait_first()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
@@ -975,14 +1034,21 @@ def run_serving(args):
 
     # grow the pool: every request once (or the first --serve-warm), one at a
     # time, then once served back to back
-    if args.serve_warm == 0 or args.serve_warm >= len(reqs):
+    # (all arriving at once, so the grouped form also reaches its largest
+    # groups: a group holds its members' scratch at the same time, and the
+    # pool grows, synchronously, the first time it needs more)
+    def warm():
         sequential(False)
         served(False, np.zeros(len(reqs)))
+        if args.group > 1:
+            served(False, np.zeros(len(reqs)), server_g)
+
+    if args.serve_warm == 0 or args.serve_warm >= len(reqs):
+        warm()
     else:
         full = (reqs, mats)
         reqs, mats = reqs[:args.serve_warm], mats[:args.serve_warm]
-        sequential(False)
-        served(False, np.zeros(len(reqs)))
+        warm()
         reqs, mats = full
     seq_s, seq_lat = sequential(False)
     plain_s, plain_lat = sequential(True)
