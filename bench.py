@@ -985,7 +985,7 @@ def run_serving(args):
     mats = [views(f, shapes, 7 * i + 1) for i, (f, b, shapes) in enumerate(reqs)]
     cells = [sum(w << lh for lh, w in shapes) for (_, _, shapes) in reqs]
     total_cells = sum(cells)
-    ctx = GpuContext(0, n_streams=8, max_inflight=args.slots)
+    ctx = GpuContext(0, n_streams=8, max_inflight=args.slots, max_group=1)  # each request alone
     server = CommitServer(ctx)
     # the grouped form's context shares the device's memory pool and budget
     ctx_g = GpuContext(0, hbm_budget_bytes=ctx.memory()[1], n_streams=8, max_inflight=args.slots,

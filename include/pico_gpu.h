@@ -89,7 +89,7 @@ typedef struct {
   uint32_t max_inflight;     /* serving: requests on the device at once; 0 = n_streams */
   uint32_t max_group;        /* serving: queued requests admitted together as one group that shares its
                                 LDE and row-hashing launches (batched device-input requests of one field);
-                                0 or 1 = each request alone, at most 16 */
+                                0 = 8, 1 = each request alone, at most 16 */
   uint32_t reserved[4];
 } pico_config;
 

@@ -415,7 +415,7 @@ extern "C" pico_status pico_gpu_init(int device, const pico_config* cfg, pico_ct
   ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
   const uint32_t ns = (cfg && cfg->n_streams) ? cfg->n_streams : 8;
   ctx->max_inflight = (cfg && cfg->max_inflight) ? std::min(cfg->max_inflight, ns) : ns;
-  ctx->max_group = (cfg && cfg->max_group) ? std::min<uint32_t>(cfg->max_group, kMaxGroup) : 1;
+  ctx->max_group = (cfg && cfg->max_group) ? std::min<uint32_t>(cfg->max_group, kMaxGroup) : kDefaultGroup;
   for (uint32_t i = 0; i < ns; i++) {
     cudaStream_t st, cst;
     if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"))) return s;

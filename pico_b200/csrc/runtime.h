@@ -62,7 +62,8 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
                         CommitPlan& plan, uint32_t shard_log = 0, uint32_t shard = 0);
 
 struct Server;  // serving.h
-constexpr uint32_t kMaxGroup = 16;  // serving: largest group of requests sharing launches
+constexpr uint32_t kMaxGroup = 16;     // serving: largest group of requests sharing launches
+constexpr uint32_t kDefaultGroup = 8;  // pico_config.max_group = 0
 
 // Stream-ordered device allocation of the library (failure injection for
 // tests included); free with cudaFreeAsync on a stream ordered after st.
@@ -122,7 +123,7 @@ struct pico_ctx {
   pico::GuardRecord* guard_host = nullptr;  // pinned: 2 records (LDE, hashing) per stream slot
   pico::Server* server = nullptr;
   uint32_t max_inflight = 0;  // serving: requests on the device at once
-  uint32_t max_group = 1;     // serving: requests admitted together into one slot (shared launches)
+  uint32_t max_group = pico::kDefaultGroup;  // serving: requests admitted together into one slot (shared launches)
   // Autotuned choices (pico_gpu_autotune), per field: the LDE's four-step
   // split log2 n1 per height (0 = default) and the row-hashing block size.
   uint8_t lde_split[2][pico::kLdeMaxLogN + 1] = {};
