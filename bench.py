@@ -164,6 +164,7 @@ LDE_TRAFFIC_RATIO = 2305 / 805
 
 
 GOLDEN_ROOTS = ROOT / "tests" / "golden" / "config_roots.json"
+DEFAULT_WORKLOAD = "uneven-kb-2^30"
 
 
 def root_parity(workload: str, seed: int, roots: dict) -> dict:
@@ -507,8 +508,59 @@ def run_gpu(args, rank, world, local):
     if ms_plain is not None:
         result["plain_form"] = {"value": world * cells * args.steps / (ms_plain / 1e3),
                                 "ms_per_step": ms_plain / args.steps}
+    if args.workload == DEFAULT_WORKLOAD and world == 1 and not args.skip_c1:
+        result["c1"] = c1_summary(ctx, args, local)
     ctx.close()
     return result, shapes, field, b
+
+
+C1_WORKLOAD = "single-kb-2^16x64"
+C1_STEPS = 50
+
+
+def c1_summary(ctx, args, local):
+    """The single-matrix KoalaBear commit (2^16 x 64, blowup 2): device-resident
+    and end-to-end rates over C1_STEPS commits each, the CPU oracle on the same
+    whole commit (all host threads, median of 5), the ratios, and the root
+    against the oracle's golden."""
+    import torch
+
+    from pico_b200 import TwoAdicDomain, TwoAdicFriPcs
+    from pico_b200 import fields as F
+
+    wl = WORKLOADS[C1_WORKLOAD]
+    field, b, shapes, seed = wl["field"], wl["log_blowup"], wl["shapes"](), wl["seed"]
+    dev = torch.device("cuda", local)
+    traces = [F.random_matrix_torch(field, lh, w, seed * 1000 + i, dev) for i, (lh, w) in enumerate(shapes)]
+    host = [t.cpu().pin_memory().numpy().view(np.uint32) for t in traces]
+    cells = sum(w << lh for lh, w in shapes)
+    pcs = TwoAdicFriPcs(ctx, field, b)
+    doms = [TwoAdicDomain(lh) for lh, _ in shapes]
+    out = {}
+    for tag, inputs in (("device", traces), ("host", host)):
+        for _ in range(max(args.warmup, 3)):
+            pcs.commit(list(zip(doms, inputs)), keep=False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(C1_STEPS):
+            root, _ = pcs.commit(list(zip(doms, inputs)), keep=False)
+        e1.record()
+        e1.synchronize()
+        out[tag] = (e0.elapsed_time(e1) / C1_STEPS, root.tolist())
+    cpu = run_cpu(shapes, field, b, seed, 5, 1, max_cells=cells)
+    ms_dev, ms_e2e = out["device"][0], out["host"][0]
+    return {
+        "workload": C1_WORKLOAD, "trace_cells": cells, "log_blowup": b, "steps": C1_STEPS,
+        "value": cells / (ms_dev / 1e3), "ms_per_step": ms_dev,
+        "e2e": {"value": cells / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 32},
+        "cpu_baseline": cpu,
+        "gpu_over_cpu": cells / (ms_dev / 1e3) / cpu["value"],
+        "gpu_over_cpu_e2e": cells / (ms_e2e / 1e3) / cpu["value"],
+        "parity": root_parity(C1_WORKLOAD, seed, {tag: r for tag, (_, r) in out.items()}),
+        "l2": "input 16 MiB, LDE 32 MiB: smaller than L2, not flushed (the size the config names)",
+    }
 
 
 # ---------------------------------------------------------------- opening leg
@@ -1102,7 +1154,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS) + ["fri-kb-2^23", "serving", "quotient-kb-2^20"]
                     + list(OPEN_WORKLOADS),
-                    default="uneven-kb-2^30")
+                    default=DEFAULT_WORKLOAD)
     ap.add_argument("--requests", type=int, default=60, help="serving: number of requests")
     ap.add_argument("--load", type=float, default=0.8,
                     help="serving: offered load vs the plain form's one-at-a-time capacity")
@@ -1122,6 +1174,7 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-lde", action="store_true", help="skip the LDE-alone timing")
+    ap.add_argument("--skip-c1", action="store_true", help="skip the single-matrix (2^16 x 64) summary key")
     ap.add_argument("--no-tune", action="store_true", help="default LDE splits and block size (no autotuning)")
     args = ap.parse_args()
 
