@@ -232,8 +232,10 @@ pico_status pico_gpu_mmcs_commit(pico_ctx *ctx, pico_field field, const pico_mat
  * their heights meet, as in the full tree); that tree is the full tree's
  * subtree under the node at depth k, index s, and `root` receives it.
  * pico_gpu_merkle_top turns the 2^k shard roots into the commitment root.  The
- * prover data holds the shard's rows (lde_rows and the digest layers count
- * them from the shard's first row). */
+ * prover data holds the shard's rows (lde_rows, digest_layer and open_batch
+ * count them from the shard's first row); the calls that need every committed
+ * row (pcs_open, open_values, reduced_opening, evaluations_on_domain,
+ * quotient_values) refuse it with PICO_ERR_UNSUPPORTED. */
 pico_status pico_gpu_commit_shard(pico_ctx *ctx, pico_field field, const pico_matrix *mats, uint32_t n_mats,
                                   uint32_t log_blowup, uint32_t log_shards, uint32_t shard, uint32_t flags,
                                   pico_commit **out, uint32_t root[8]);

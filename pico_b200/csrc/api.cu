@@ -782,6 +782,7 @@ static pico_status setup_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStrea
   c->field = field;
   c->log_max = plan.log_max;
   c->n_mats = n;
+  c->shard_log = plan.shard_log;
   c->lde.assign(n, nullptr);
   c->log_N.assign(n, 0);
   c->width.assign(n, 0);

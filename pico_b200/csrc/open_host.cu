@@ -57,6 +57,10 @@ pico_status check_batches(pico_ctx* ctx, const pico_open_batch* b, uint32_t n, u
       set_error("open: batch %u has no commitment of this context", i);
       return PICO_ERR_INVALID_ARG;
     }
+    if (c->shard_log) {
+      set_error("open: batch %u is one shard of a row-split commit; it holds a slice of the committed rows", i);
+      return PICO_ERR_UNSUPPORTED;
+    }
     if (sh.field < 0) sh.field = c->field;
     if (c->field != sh.field) {
       set_error("open: batches of different fields");
@@ -930,6 +934,10 @@ extern "C" pico_status pico_gpu_evaluations_on_domain(pico_ctx* ctx, const pico_
   if (!ctx || !c || c->ctx != ctx || !out || mat_idx >= c->n_mats) {
     set_error("evaluations_on_domain: bad arguments");
     return PICO_ERR_INVALID_ARG;
+  }
+  if (c->shard_log) {
+    set_error("evaluations_on_domain: the commitment is one shard of a row-split commit");
+    return PICO_ERR_UNSUPPORTED;
   }
   if (log_domain > c->log_N[mat_idx]) {
     set_error("evaluations_on_domain: domain 2^%u is taller than the committed LDE 2^%u", log_domain,

@@ -168,6 +168,10 @@ pico_status trace_view(pico_ctx* ctx, const pico_trace_ref& r, int field, uint32
     set_error("quotient_values: the %s trace is not a matrix of a commit of this context and field", what);
     return PICO_ERR_INVALID_ARG;
   }
+  if (c->shard_log) {
+    set_error("quotient_values: the %s trace's commitment is one shard of a row-split commit", what);
+    return PICO_ERR_UNSUPPORTED;
+  }
   if (c->log_N[r.mat_idx] < log_q) {
     set_error("quotient_values: the %s LDE has 2^%u rows, fewer than the quotient domain's 2^%u", what,
               c->log_N[r.mat_idx], log_q);

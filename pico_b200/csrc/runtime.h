@@ -142,6 +142,7 @@ struct pico_commit {
   std::vector<uint32_t> width;    // per input index
   std::vector<void*> blocks;      // the commit's device allocations: owned LDEs / copied inputs, layers
   uint32_t* layers = nullptr;     // all digest layers, leaves first (in one of the blocks)
+  uint32_t shard_log = 0;         // > 0: one shard of a row-split commit (pico_gpu_commit_shard)
   uint64_t bytes_resident = 0;
   uint32_t root[8] = {0};
   // events (see finish_stats): compute-stream phases 0, 3, 4, copy stream 5..6,

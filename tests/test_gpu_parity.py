@@ -11,6 +11,7 @@ import pytest
 
 from pico_b200 import (CommitServer, GpuContext, MerkleTreeMmcs, PicoError, Poseidon2, Radix2DitParallel,
                        TwoAdicDomain, TwoAdicFriPcs)
+from pico_b200 import abi
 from pico_b200 import fields as F
 
 pytestmark = pytest.mark.gpu
@@ -483,6 +484,10 @@ def test_row_split_commit(gpu, orc, f, b, k):
     for s in range(1 << k):
         sub, pd = pcs.commit_shard(list(zip(doms, mats)), k, s)
         assert sub.tolist() == depth_k[s].tolist(), s
+        if k:  # a shard holds a slice of the rows: calls that need all of them refuse it
+            with pytest.raises(PicoError) as e:
+                pd.evaluations_on_domain(0, shapes[0][0])
+            assert e.value.status == abi.PICO_ERR_UNSUPPORTED
         for i, l in enumerate(ldes):
             rows = l.shape[0] >> k
             assert pd.lde_shape(i) == (rows, l.shape[1])
