@@ -136,6 +136,15 @@ const char *pico_gpu_last_error(void);
 uint32_t pico_gpu_abi_version(void);
 /* Bytes currently reserved by resident commits / in-flight requests, and the budget. */
 pico_status pico_gpu_memory(pico_ctx *ctx, uint64_t *reserved, uint64_t *budget);
+/* Grow the device's stream-ordered memory pool, which every device buffer of
+ * this library comes from, to hold at least `bytes` (at most the context's
+ * budget) by allocating and freeing that much once, so that later commits and
+ * served requests take memory from the pool instead of growing it: growth is
+ * synchronous, and the first group of served requests that needed more than
+ * the pool held stalled for up to 0.3 s in measurement.  The pool keeps its
+ * memory until the process exits (other allocators of the process cannot use
+ * it).  pool_bytes (nullable) receives what the pool then holds. */
+pico_status pico_gpu_reserve_pool(pico_ctx *ctx, uint64_t bytes, uint64_t *pool_bytes);
 /* Device bytes a commit of these matrices would reserve against the budget
  * (pico_gpu_commit / pico_gpu_submit_commit with the same arguments):
  * `resident` stays reserved until the commit is released (LDEs, digest

@@ -148,6 +148,7 @@ SIGNATURES = {
     "pico_gpu_last_error": (C.c_char_p, []),
     "pico_gpu_abi_version": (_u32, []),
     "pico_gpu_memory": (C.c_int, [_vp, C.POINTER(_u64), C.POINTER(_u64)]),
+    "pico_gpu_reserve_pool": (C.c_int, [_vp, _u64, C.POINTER(C.c_uint64)]),
     "pico_gpu_commit_bytes": (C.c_int, [C.c_int, C.POINTER(Matrix), _u32, _u32, _u32, C.POINTER(_u64),
                                         C.POINTER(_u64)]),
     "pico_gpu_commit": (C.c_int, [_vp, C.c_int, C.POINTER(Matrix), _u32, _u32, _u32, C.POINTER(_vp), _u32p]),

@@ -511,6 +511,33 @@ extern "C" pico_status pico_gpu_memory(pico_ctx* ctx, uint64_t* reserved, uint64
   return PICO_OK;
 }
 
+extern "C" pico_status pico_gpu_reserve_pool(pico_ctx* ctx, uint64_t bytes, uint64_t* pool_bytes) {
+  if (!ctx) {
+    set_error("reserve_pool: null context");
+    return PICO_ERR_INVALID_ARG;
+  }
+  pico_status s;
+  if ((s = cuda_status(cudaSetDevice(ctx->device), "cudaSetDevice"))) return s;
+  cudaMemPool_t pool;
+  if ((s = cuda_status(cudaDeviceGetDefaultMemPool(&pool, ctx->device), "cudaDeviceGetDefaultMemPool"))) return s;
+  bytes = std::min<uint64_t>(bytes, ctx->budget);
+  if (bytes) {
+    // one allocation of the whole amount, freed at once: the pool keeps it
+    // (release threshold unlimited) and splits it for later allocations
+    cudaStream_t st = aux_stream(ctx);
+    void* p = nullptr;
+    if ((s = device_alloc(&p, bytes, st))) return s;
+    if ((s = cuda_status(cudaFreeAsync(p, st), "pool reservation"))) return s;
+    if ((s = cuda_status(cudaStreamSynchronize(st), "pool reservation"))) return s;
+  }
+  if (pool_bytes) {
+    uint64_t v = 0;  // the attribute is a 64-bit value
+    if ((s = cuda_status(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v), "pool size"))) return s;
+    *pool_bytes = (uint64_t)v;
+  }
+  return PICO_OK;
+}
+
 namespace pico {
 
 bool try_reserve(pico_ctx* ctx, uint64_t bytes) {

@@ -72,6 +72,13 @@ class GpuContext:
         abi.check(self.lib.pico_gpu_memory(self.handle, C.byref(r), C.byref(b)))
         return r.value, b.value
 
+    def reserve_pool(self, nbytes: int) -> int:
+        """Grow the device memory pool to hold at least nbytes (pico_gpu_reserve_pool);
+        returns the bytes the pool then holds."""
+        out = C.c_uint64()
+        abi.check(self.lib.pico_gpu_reserve_pool(self.handle, nbytes, C.byref(out)))
+        return out.value
+
     def autotune(self, field, log_n_min: int = 12, log_n_max: int = 22) -> dict:
         """Time the LDE's four-step splits per height and the row-hashing block
         size on this device and keep the fastest (pico_gpu_autotune).  Returns

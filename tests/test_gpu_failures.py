@@ -146,3 +146,22 @@ def test_context_stays_usable_after_refused_calls(gpu, orc):
     want = orc.pcs_commit(0, [m], [F.lde_shift(0)], 1)[0]
     got, _ = TwoAdicFriPcs(gpu, 0, 1).commit([(TwoAdicDomain(8), m)], keep=False)
     assert got.tolist() == want.tolist()
+
+
+def test_reserve_pool_grows_the_pool_and_reports_failures(gpu):
+    """pico_gpu_reserve_pool: the pool holds at least what was asked, the
+    budget accounting is untouched, and an allocation failure on the way is
+    reported as PICO_ERR_OUT_OF_MEMORY with the context still usable."""
+    lib = abi.load()
+    before = gpu.reserve_pool(0)
+    after = gpu.reserve_pool(before + (256 << 20))
+    assert after >= before + (256 << 20)
+    assert gpu.memory()[0] == 0
+    lib.pico_gpu_test_fail_allocations(0)
+    try:
+        with pytest.raises(PicoError) as e:
+            gpu.reserve_pool(after + (64 << 20))
+        assert e.value.status == abi.PICO_ERR_OUT_OF_MEMORY
+    finally:
+        lib.pico_gpu_test_fail_allocations(-1)
+    assert gpu.reserve_pool(0) >= after
