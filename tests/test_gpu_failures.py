@@ -165,3 +165,57 @@ def test_reserve_pool_grows_the_pool_and_reports_failures(gpu):
     finally:
         lib.pico_gpu_test_fail_allocations(-1)
     assert gpu.reserve_pool(0) >= after
+
+
+def test_grouped_requests_survive_an_allocation_failure(orc):
+    """An allocation that fails while device-input requests are admitted as a
+    group: every request either finishes with its oracle root or reports
+    PICO_ERR_OUT_OF_MEMORY, every reserved byte comes back, and the next
+    group is bit-exact.  (Which request meets the failure depends on timing;
+    the outcome rules do not.)"""
+    import time
+
+    import torch
+
+    lib = abi.load()
+    f, b = 0, 1
+    big = torch.from_numpy(F.random_matrix(f, 22, 64, 2600).view(np.int32)).cuda()
+    small = [mats_of(f, [(9 + i, 5), (7, 3)], 2610 + 10 * i) for i in range(4)]
+    want = [orc.pcs_commit(f, m, [F.lde_shift(f)] * 2, b)[0] for m in small]
+    dev = [[torch.from_numpy(x.view(np.int32)).cuda() for x in m] for m in small]
+    with GpuContext(0, n_streams=2, max_inflight=1, max_group=8) as ctx:
+        server = CommitServer(ctx)
+        first = server.submit(f, [big], b)  # holds the only slot while the others queue
+        time.sleep(0.05)
+        lib.pico_gpu_test_fail_allocations(0)
+        try:
+            reqs = [server.submit(f, d, b) for d in dev]
+            failed = 0
+            try:
+                first.wait(timeout_ms=120_000, keep=False)
+            except PicoError as e:
+                assert e.status == abi.PICO_ERR_OUT_OF_MEMORY
+                failed += 1
+            for r, w in zip(reqs, want):
+                try:
+                    root, _ = r.wait(timeout_ms=120_000, keep=False)
+                    assert root.tolist() == w.tolist()
+                except PicoError as e:
+                    assert e.status == abi.PICO_ERR_OUT_OF_MEMORY
+                    failed += 1
+                r.free()
+            assert failed >= 1  # the one injected failure reached a request (a group fails whole)
+        finally:
+            lib.pico_gpu_test_fail_allocations(-1)
+        first.free()
+        assert ctx.memory()[0] == 0
+        # the same requests again, after the injection: all bit-exact
+        first = server.submit(f, [big], b)
+        reqs = [server.submit(f, d, b) for d in dev]
+        first.wait(timeout_ms=120_000, keep=False)
+        for r, w in zip(reqs, want):
+            root, _ = r.wait(timeout_ms=120_000, keep=False)
+            assert root.tolist() == w.tolist()
+            r.free()
+        first.free()
+        assert ctx.memory()[0] == 0
