@@ -516,3 +516,30 @@ def test_row_split_commit_device_inputs_at_2_20(gpu, orc):
     want, _, _ = orc.pcs_commit(f, host, [F.lde_shift(f)] * 2, b)
     subs = [pcs.commit_shard(list(zip(doms, dev)), 1, s, keep=False)[0] for s in range(2)]
     assert merkle_top(f, np.stack(subs)).tolist() == want.tolist()
+
+
+def test_commit_sharded_over_a_one_rank_group(orc, tmp_path):
+    """pico_b200.sharded.commit_sharded on a one-rank gloo group (this GPU is
+    shard 0 of 1): the product path end to end, all-gather included."""
+    import socket
+
+    import torch.distributed as dist
+
+    from pico_b200.sharded import commit_sharded
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    ctx = GpuContext(0)
+    try:
+        f, b = 1, 2
+        mats = [F.random_matrix(f, lh, w, 9300 + lh) for lh, w in ((12, 6), (10, 3))]
+        pcs = TwoAdicFriPcs(ctx, f, b)
+        root, pd, sub = commit_sharded(pcs, [(TwoAdicDomain(m.shape[0].bit_length() - 1), m) for m in mats])
+        want, _, _ = orc.pcs_commit(f, mats, [F.lde_shift(f)] * 2, b)
+        assert root.tolist() == sub.tolist() == want.tolist()
+        pd.release()
+    finally:
+        ctx.close()
+        dist.destroy_process_group()
