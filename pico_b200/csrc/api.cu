@@ -670,10 +670,6 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
   for (uint32_t i = 0; i < n;) {
     uint32_t j = i;
     while (j < n && plan.mats[j].log_N == plan.mats[i].log_N) j++;
-    if (j - i > (uint32_t)kMaxSegs) {
-      set_error("commit: %u matrices share height 2^%u (max %d)", j - i, plan.mats[i].log_N, kMaxSegs);
-      return PICO_ERR_UNSUPPORTED;
-    }
     plan.groups.push_back({i, j});
     i = j;
   }
@@ -706,7 +702,12 @@ pico_status plan_commit(int field, const pico_matrix* mats, uint32_t n, uint32_t
     }
     const uint64_t rows = 1ull << plan.mats[plan.groups[gi].first].log_N;
     if (gi > 0) scr += rows * 32;  // injected-row digests
-    if ((!plan.input_device || plan.plain) && nonzero >= 2) state_rows = std::max(state_rows, rows);
+    // a group hashed matrix by matrix (resumable sponge) keeps row states:
+    // host inputs and the plain form, and any group of more matrices with
+    // columns than one row-hashing launch takes (kMaxSegs)
+    if (nonzero > (uint32_t)kMaxSegs) plan.wide_groups = true;
+    if (((!plan.input_device || plan.plain) && nonzero >= 2) || nonzero > (uint32_t)kMaxSegs)
+      state_rows = std::max(state_rows, rows);
     const uint64_t absorb = rows * ((wsum + 7) / 8);
     if (gi == 0)
       plan.leaf_permutations = absorb;
@@ -860,7 +861,8 @@ static pico_status setup_commit(pico_ctx* ctx, const CommitPlan& plan, cudaStrea
   chained.assign(G, false);
   uint64_t rows_max = 0;
   for (uint32_t gi = 0; gi < G; gi++) {
-    chained[gi] = (copy_in || plan.plain) && nonzero_mats(plan, gi) >= 2;
+    const uint32_t nz = nonzero_mats(plan, gi);
+    chained[gi] = ((copy_in || plan.plain) && nz >= 2) || nz > (uint32_t)kMaxSegs;
     if (chained[gi]) rows_max = std::max<uint64_t>(rows_max, 1ull << plan.mats[plan.groups[gi].first].log_N);
   }
   const uint32_t nb = 1u << (plan.log_b - plan.shard_log);  // coset blocks per LDE
@@ -1217,8 +1219,9 @@ pico_status enqueue_commit_group(pico_ctx* ctx, const std::vector<const CommitPl
   }
   const int field = plans[0]->field;
   for (const CommitPlan* p : plans)
-    if (p->field != field || !p->input_device || !p->extend || p->plain) {
-      set_error("commit group: members must share the field and be extended batched commits of device inputs");
+    if (p->field != field || !p->input_device || !p->extend || p->plain || p->wide_groups) {
+      set_error("commit group: members must share the field and be extended batched commits of device inputs "
+                "with at most %d matrices of columns per height", kMaxSegs);
       return PICO_ERR_INVALID_ARG;
     }
   pico_status s;

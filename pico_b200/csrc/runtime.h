@@ -42,6 +42,7 @@ struct CommitPlan {
   bool extend = true;            // false: mmcs_commit of already-extended matrices
   bool input_device = false;
   bool plain = false;
+  bool wide_groups = false;      // a height group has more matrices with columns than kMaxSegs
   std::vector<PlannedMat> mats;  // in commit order (stable, tallest first)
   // height groups in commit order: [begin, end) into mats
   std::vector<std::pair<uint32_t, uint32_t>> groups;

@@ -76,7 +76,7 @@ struct Server {
   bool admit(pico_request* r);
   void fill_group(Group* g, Clock::time_point now);
   bool groupable(const pico_request* r) const {
-    return ctx->max_group > 1 && r->plan.input_device && r->plan.extend && !r->plan.plain;
+    return ctx->max_group > 1 && r->plan.input_device && r->plan.extend && !r->plan.plain && !r->plan.wide_groups;
   }
 };
 

@@ -543,3 +543,29 @@ def test_commit_sharded_over_a_one_rank_group(orc, tmp_path):
     finally:
         ctx.close()
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dev_in", [False, True])
+@pytest.mark.parametrize("plain", [False, True])
+def test_commit_with_more_matrices_per_height_than_one_launch(gpu, orc, dev_in, plain):
+    """70 matrices of one height (more than the 64 segments one row-hashing
+    launch concatenates) plus a shorter group: that height's rows are absorbed
+    matrix by matrix through the resumable sponge, bit-exact with the oracle;
+    served, such a request runs alone."""
+    f, b = 0, 1
+    shapes = [(6, 1 + i % 3) for i in range(70)] + [(4, 2), (6, 0)]
+    mats = [F.random_matrix(f, lh, w, 9500 + i) for i, (lh, w) in enumerate(shapes)]
+    want, _, _ = orc.pcs_commit(f, mats, [F.lde_shift(f)] * len(mats), b)
+    inputs = mats
+    if dev_in:
+        torch = _torch()
+        inputs = [torch.from_numpy(m.view(np.int32)).cuda() for m in mats]
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    root, _ = pcs.commit([(TwoAdicDomain(lh), m) for (lh, _), m in zip(shapes, inputs)], plain=plain, keep=False)
+    assert root.tolist() == want.tolist()
+    if not plain:
+        req = CommitServer(gpu).submit(f, inputs, b)
+        got, _ = req.wait(timeout_ms=60_000, keep=False)
+        req.free()
+        assert got.tolist() == want.tolist()
+    assert gpu.memory()[0] == 0
