@@ -57,6 +57,7 @@ typedef enum { PICO_KOALABEAR = 0, PICO_BABYBEAR = 1 } pico_field;
 #define PICO_OUTPUT_DEVICE 0x4u /* output pointers are device pointers (else host) */
 #define PICO_LDE_NATURAL_ORDER 0x8u /* coset_lde_batch: natural row order (Dft trait); default bit-reversed */
 #define PICO_P2_FOUR_LANES 0x10u /* poseidon2_permute: four threads per state (shorter latency per state) */
+#define PICO_QUOTIENT_CHUNKS 0x20u /* quotient_values: output split into its 2^log_quotient_degree chunks */
 
 typedef struct pico_ctx pico_ctx;
 /* Prover data of one commit: every LDE and every digest layer stays resident
@@ -367,7 +368,13 @@ pico_status pico_gpu_reduced_opening(pico_ctx *ctx, const pico_open_batch *batch
  * b = 1 reads the next row.  Constants are Monty form.  public_values (n_public
  * words), perm_challenges (n_challenges x 4), regional_sum (4, nullable),
  * global_sum (14 coordinates of the septic digest, nullable), alpha (4).
- * out: Q x 4 words, host memory unless PICO_OUTPUT_DEVICE.  No counterpart in
+ * out: Q x 4 words, host memory unless PICO_OUTPUT_DEVICE.  With
+ * PICO_QUOTIENT_CHUNKS the output is the D = 2^log_quotient_degree chunks
+ * that the prover commits next (prover.rs:517-538: flatten_to_base, then the
+ * domain's split_evals and split_domains): chunk j, n = 2^log_trace_height
+ * EF4 values at out + 4 n j, holds the points i = j, j + D, j + 2D, ..., the
+ * evaluations on GENERATOR * w_Q^j * <w_n>, so each chunk commits as a
+ * PICO_MATRIX_EXT4 matrix of height n and LDE shift w_Q^-j.  No counterpart in
  * the reference's types for the program itself: the reference evaluates the
  * Rust `eval` directly. */
 typedef enum {

@@ -40,6 +40,7 @@ PICO_COMMIT_PLAIN = 0x2
 PICO_OUTPUT_DEVICE = 0x4
 PICO_LDE_NATURAL_ORDER = 0x8
 PICO_P2_FOUR_LANES = 0x10
+PICO_QUOTIENT_CHUNKS = 0x20
 
 
 class PicoError(RuntimeError):

@@ -45,6 +45,7 @@ struct QuotientArgs {
   const uint32_t* consts;   // regional sum (4), global sum (14), alpha (4)
   uint32_t log_trace, log_qd;
   uint32_t n_base;          // base registers the program uses; the extension registers follow them
+  uint32_t chunks;          // 1: point i at out row (i mod D) n + i / D (split_evals order); 0: row i
   uint32_t* out;            // Q x 4
 };
 
@@ -140,7 +141,9 @@ __global__ void __launch_bounds__(kQThreads) k_quotient(const __grid_constant__ 
   if (active) {
     const uint4 q = make_uint4(B::mul(acc.c[0], inv_zh), B::mul(acc.c[1], inv_zh), B::mul(acc.c[2], inv_zh),
                                B::mul(acc.c[3], inv_zh));
-    reinterpret_cast<uint4*>(A.out)[i] = q;
+    const uint64_t orow =
+        A.chunks ? ((i & ((1ull << A.log_qd) - 1)) << A.log_trace) + (i >> A.log_qd) : i;  // a permutation of [0, Q)
+    reinterpret_cast<uint4*>(A.out)[orow] = q;
   }
 }
 
@@ -196,7 +199,7 @@ extern "C" pico_status pico_gpu_quotient_values(pico_ctx* ctx, pico_trace_ref pr
     set_error("quotient_values: null argument");
     return PICO_ERR_INVALID_ARG;
   }
-  if (flags & ~PICO_OUTPUT_DEVICE) {
+  if (flags & ~(PICO_OUTPUT_DEVICE | PICO_QUOTIENT_CHUNKS)) {
     set_error("quotient_values: unknown flags 0x%x", flags);
     return PICO_ERR_INVALID_ARG;
   }
@@ -309,6 +312,7 @@ extern "C" pico_status pico_gpu_quotient_values(pico_ctx* ctx, pico_trace_ref pr
   A.log_trace = log_trace_height;
   A.log_qd = log_quotient_degree;
   A.n_base = n_base;
+  A.chunks = (flags & PICO_QUOTIENT_CHUNKS) ? 1u : 0u;
   A.out = out_dev ? out : blk + off_out;
   const TwiddleTables tw = twiddles(ctx, field);
   const unsigned grid = (unsigned)((Q + kQThreads - 1) / kQThreads);

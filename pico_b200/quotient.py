@@ -204,14 +204,17 @@ class ConstraintBuilder:
 
 def compute_quotient_values(ctx, program: np.ndarray, log_trace: int, log_quotient_degree: int, main,
                             preprocessed=None, permutation=None, public_values=(), perm_challenges=None,
-                            regional_sum=None, global_sum=None, alpha=None, out=None):
+                            regional_sum=None, global_sum=None, alpha=None, out=None, chunks: bool = False):
     """pico_gpu_quotient_values: the chip's quotient on the quotient domain
     GENERATOR * <w_Q>, Q = 2^(log_trace + log_quotient_degree), natural order,
     (Q, 4) Monty words.  main / preprocessed / permutation are (ProverData,
     matrix index) pairs of resident commits (None: absent), committed with
     the standard LDE shift and a blowup >= log_quotient_degree.  `out`: a
     device tensor of Q x 4 int32 to fill in place, else a host array is
-    returned."""
+    returned.  chunks=True (PICO_QUOTIENT_CHUNKS): the output is the
+    2^log_quotient_degree chunks split_evals makes, chunk j (rows j n ..
+    (j + 1) n) holding points j, j + D, ...; a host result is then shaped
+    (D, n, 4), ready for commit_quotient_chunks."""
     from .pcs import _is_device
 
     lib = ctx.lib
@@ -232,7 +235,7 @@ def compute_quotient_values(ctx, program: np.ndarray, log_trace: int, log_quotie
     glob = np.ascontiguousarray(np.zeros(14, np.uint32) if global_sum is None else global_sum, dtype=np.uint32)
     al = np.ascontiguousarray(alpha, dtype=np.uint32)
     Q = 1 << (log_trace + log_quotient_degree)
-    flags = 0
+    flags = abi.PICO_QUOTIENT_CHUNKS if chunks else 0
     if out is None:
         host = np.zeros((Q, 4), dtype=np.uint32)
         optr = host.ctypes.data
@@ -246,4 +249,27 @@ def compute_quotient_values(ctx, program: np.ndarray, log_trace: int, log_quotie
         prog.ctypes.data, prog.shape[0], pub.ctypes.data if pub.size else None, pub.size,
         chal.ctypes.data if chal.size else None, chal.shape[0], reg.ctypes.data, glob.ctypes.data, al.ctypes.data,
         optr, flags))
-    return host if out is None else out
+    if out is not None:
+        return out
+    return host.reshape(1 << log_quotient_degree, 1 << log_trace, 4) if chunks else host
+
+
+def quotient_chunk_domains(field, log_trace: int, log_quotient_degree: int):
+    """The chunks' domains (split_domains of the quotient domain GENERATOR * <w_Q>):
+    chunk j lives on GENERATOR * w_Q^j * <w_n>."""
+    from .pcs import TwoAdicDomain
+
+    f = F.field_id(field)
+    p = F.P[f]
+    wq = F.two_adic_generator(f, log_trace + log_quotient_degree)
+    return [TwoAdicDomain(log_trace, F.GENERATOR[f] * pow(wq, j, p) % p) for j in range(1 << log_quotient_degree)]
+
+
+def commit_quotient_chunks(pcs, chunks, log_trace: int, log_quotient_degree: int, keep: bool = True):
+    """Commit a chip's quotient chunks as the prover does after
+    compute_quotient_values (vm/src/machine/prover.rs:513-538): chunk j, n EF4
+    values (host (n, 4) arrays or device tensors, e.g. views of a chunked
+    output), on its split domain, as an extension matrix."""
+    doms = quotient_chunk_domains(pcs.field, log_trace, log_quotient_degree)
+    traces = [c.reshape(1 << log_trace, 1, 4) for c in chunks]
+    return pcs.commit(list(zip(doms, traces)), keep=keep)

@@ -569,3 +569,21 @@ def test_commit_with_more_matrices_per_height_than_one_launch(gpu, orc, dev_in, 
         req.free()
         assert got.tolist() == want.tolist()
     assert gpu.memory()[0] == 0
+
+
+@pytest.mark.parametrize("f", FIELDS)
+def test_row_split_commit_with_extension_traces(gpu, orc, f):
+    """A permutation trace of EF4 elements in a row-split commit: each shard
+    holds its rows of the flattened (4w-column) LDE, and the shard roots
+    combine to the root of the flattened commit."""
+    from pico_b200.pcs import merkle_top
+
+    b, k = 2, 2
+    ext = F.random_matrix(f, 9, 12, 9600 + f).reshape(1 << 9, 3, 4)
+    base = F.random_matrix(f, 10, 5, 9610 + f)
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    items = [(pcs.natural_domain_for_degree(1 << 10), base), (pcs.natural_domain_for_degree(1 << 9), ext)]
+    flat = [base, np.ascontiguousarray(ext.reshape(1 << 9, 12))]
+    want, _, _ = orc.pcs_commit(f, flat, [F.lde_shift(f)] * 2, b)
+    subs = [pcs.commit_shard(items, k, s, keep=False)[0] for s in range(1 << k)]
+    assert merkle_top(f, np.stack(subs)).tolist() == want.tolist()

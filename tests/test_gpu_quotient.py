@@ -174,3 +174,36 @@ def test_device_output_and_refusals(gpu, orc):
     with pytest.raises(PicoError):
         compute_quotient_values(gpu, bad, logn, log_qd, (pd, 0), alpha=alpha)
     pd.release()
+
+
+@pytest.mark.parametrize("f", FIELDS)
+@pytest.mark.parametrize("log_qd", [1, 2])
+def test_quotient_chunks_commit_as_the_prover_does(gpu, orc, f, log_qd):
+    """PICO_QUOTIENT_CHUNKS: chunk j holds points j, j + D, ... (split_evals);
+    committed on their split domains (prover.rs:513-538), the root is the
+    oracle's commit of the same chunks with shifts GENERATOR / (GENERATOR w_Q^j)."""
+    from pico_b200.quotient import commit_quotient_chunks, quotient_chunk_domains
+
+    logn, b = 8, log_qd
+    bld = ConstraintBuilder()
+    x, y = bld.main(0), bld.main(1)
+    bld.when_transition().assert_eq(bld.main(0, True), y)
+    bld.when_transition().assert_eq(bld.main(1, True), x * y)
+    prog = bld.program(f)
+    main = F.random_matrix(f, logn, 2, 8700 + f)
+    alpha = rand_ext(f, 1, 8710 + f)[0]
+    pd = commit(gpu, f, b, [main])
+    nat = compute_quotient_values(gpu, prog, logn, log_qd, (pd, 0), alpha=alpha)
+    ch = compute_quotient_values(gpu, prog, logn, log_qd, (pd, 0), alpha=alpha, chunks=True)
+    D = 1 << log_qd
+    assert ch.shape == (D, 1 << logn, 4)
+    for j in range(D):
+        assert (ch[j] == nat[j::D]).all()
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    root, qpd = commit_quotient_chunks(pcs, [ch[j] for j in range(D)], logn, log_qd)
+    doms = quotient_chunk_domains(f, logn, log_qd)
+    want, _, _ = orc.pcs_commit(f, [np.ascontiguousarray(ch[j]) for j in range(D)],
+                                [F.lde_shift(f, d.shift) for d in doms], b)
+    assert root.tolist() == want.tolist()
+    qpd.release()
+    pd.release()
