@@ -499,6 +499,9 @@ def test_row_split_commit(gpu, orc, f, b, k):
     pd_full.release()
     with pytest.raises(PicoError):
         pcs.commit_shard(list(zip(doms, mats)), b + 1, 0, keep=False)
+    with pytest.raises(PicoError) as e:  # a shard index past the last shard
+        pcs.commit_shard(list(zip(doms, mats)), k, 1 << k, keep=False)
+    assert e.value.status == abi.PICO_ERR_INVALID_ARG
     assert gpu.memory()[0] == 0
 
 
