@@ -158,3 +158,22 @@ def test_opcodes_agree_across_header_builder_and_oracle():
         o = re.search(rf"ORC_Q_{name} = (\d+)", oracle_h)
         assert m and int(m.group(1)) == v, name
         assert o and int(o.group(1)) == v, name
+
+
+def test_quotient_chunk_domains_are_the_split_domains():
+    """split_domains of GENERATOR * <w_Q> into D chunks: chunk j is
+    GENERATOR * w_Q^j * <w_n>, and its LDE shift GENERATOR / shift is w_Q^-j
+    (Monty form), the shift its chunk of PICO_QUOTIENT_CHUNKS output commits with."""
+    from pico_b200 import fields as F
+    from pico_b200.quotient import quotient_chunk_domains
+
+    for f in (0, 1):
+        p = F.P[f]
+        for log_n, log_qd in ((5, 1), (8, 2), (3, 3)):
+            wq = F.two_adic_generator(f, log_n + log_qd)
+            doms = quotient_chunk_domains(f, log_n, log_qd)
+            assert len(doms) == 1 << log_qd
+            for j, d in enumerate(doms):
+                assert d.log_n == log_n
+                assert d.shift == F.GENERATOR[f] * pow(wq, j, p) % p
+                assert F.lde_shift(f, d.shift) == F.monty(f, pow(wq, (p - 1 - j) % (p - 1), p))
