@@ -67,6 +67,8 @@ typedef struct pico_commit pico_commit;
 typedef struct pico_fri pico_fri;
 /* An asynchronous commit request (serving path). */
 typedef struct pico_request pico_request;
+/* One shard of a FRI commit phase split by rows over several devices. */
+typedef struct pico_fri_shard pico_fri_shard;
 
 typedef struct {
   const uint32_t *values; /* row-major 2^log_height x width, Monty form */
@@ -275,6 +277,27 @@ pico_status pico_gpu_fri_commit_phase(pico_ctx *ctx, pico_field field, const uin
 pico_status pico_gpu_fri_release(pico_ctx *ctx, pico_fri *f);
 /* Codeword of round r (r = 0 is the input) as 2^(log_n - r) x 4 words. */
 pico_status pico_gpu_fri_layer(pico_ctx *ctx, const pico_fri *f, uint32_t round, uint32_t *out, uint32_t flags);
+
+/* The commit phase of a codeword split by rows over 2^k devices (no
+ * counterpart in the reference, which runs it on one host).  Shard s holds
+ * rows [s N / 2^k, (s + 1) N / 2^k) of the N-row EF4 codeword (committed
+ * order, 4 words per row), the row partition of pico_gpu_commit_shard.  A
+ * round's tree hashes rows 2i, 2i + 1 into leaf i, so a shard's rows make the
+ * subtree under node s at depth k, and the fold pairs the same rows, so the
+ * next round's shard rows come from this shard's alone.  Per round the caller
+ * gathers the 2^k shard roots (pico_gpu_merkle_top gives the round's root),
+ * observes it and samples beta on its challenger, and calls fold with beta;
+ * when the shards are short it gathers the codeword (pico_gpu_fri_shard_rows)
+ * and finishes with pico_gpu_fri_commit_phase on one device, continuing the
+ * same challenger.  begin: the shard's rows (host, or device with
+ * PICO_INPUT_DEVICE) of a 2^log_n-row codeword, and its round-0 subtree root.
+ * fold: the next round's rows and subtree root (needs at least 4 rows). */
+pico_status pico_gpu_fri_shard_begin(pico_ctx *ctx, pico_field field, const uint32_t *rows, uint32_t log_n,
+                                     uint32_t log_shards, uint32_t shard, uint32_t flags, pico_fri_shard **out,
+                                     uint32_t root[8]);
+pico_status pico_gpu_fri_shard_fold(pico_fri_shard *fs, const uint32_t beta[4], uint32_t root[8]);
+pico_status pico_gpu_fri_shard_rows(pico_fri_shard *fs, uint32_t *out, uint32_t flags);
+pico_status pico_gpu_fri_shard_release(pico_fri_shard *fs);
 
 /* ---- PCS opening (TwoAdicFriPcs::open, vm/src/machine/prover.rs:589) -------
  * Every step follows the Pico verifier (vm/src/compiler/recursion/circuit/

@@ -277,3 +277,182 @@ extern "C" pico_status pico_gpu_fri_layer(pico_ctx* ctx, const pico_fri* f, uint
   if (s) return s;
   return cuda_status(cudaStreamSynchronize(st), "fri_layer");
 }
+
+// ---------------------------------------------------------------------------
+// The FRI commit phase of a codeword split by rows over 2^k devices (the row
+// partition of pico_gpu_commit_shard).  A round's tree is MerkleTreeMmcs over
+// the codeword viewed as (len/2) x 8 base words: leaf i is rows 2i, 2i + 1, so
+// shard s's rows make the subtree under node s at depth k.  The fold pairs the
+// same rows, so the next codeword's shard s rows are the fold of this shard's
+// rows: nothing crosses devices but the 8-word shard roots (and the final
+// gather of a short codeword, done by the caller).
+
+struct pico_fri_shard {
+  pico_ctx* ctx = nullptr;
+  int field = 0;
+  uint32_t log_len = 0;     // the whole codeword of the current round: 2^log_len rows
+  uint32_t log_shards = 0, shard = 0;
+  uint32_t* cw[2] = {nullptr, nullptr};  // this shard's rows of the current / next codeword
+  uint32_t cur = 0;
+  uint32_t* tree = nullptr;  // digest layers of the current round's subtree, leaves first
+  uint32_t* d_beta = nullptr;
+  void* block = nullptr;
+  uint64_t bytes = 0;
+  cudaStream_t st = nullptr;
+  uint32_t slot = 0;
+  uint32_t log_rows() const { return log_len - log_shards; }
+};
+
+namespace {
+
+// Compression levels of the current subtree (its leaves in fs->tree) up to its
+// root, then the root to the host.
+pico_status shard_tree_root(pico_fri_shard* fs, uint32_t root[8]) {
+  pico_status s;
+  const uint64_t leaves = 1ull << (fs->log_rows() - 1);
+  uint32_t* layer = fs->tree;
+  uint64_t n = leaves;
+  while (n > 512) {
+    if (n <= (1u << 15)) {
+      if ((s = cuda_status(launch_subtree(fs->field, layer, (uint32_t)n, SubtreeInj{}, fs->st), "FRI subtree")))
+        return s;
+      for (int l = 0; l < 7; l++) {
+        layer += n * 8;
+        n /= 2;
+      }
+      continue;
+    }
+    uint32_t* next = layer + n * 8;
+    if ((s = cuda_status(launch_compress(fs->field, layer, next, n / 2, nullptr, fs->st), "FRI compression")))
+      return s;
+    layer = next;
+    n /= 2;
+  }
+  if ((s = cuda_status(launch_tree_top(fs->field, layer, (uint32_t)n, nullptr, nullptr, fs->st), "FRI tree top")))
+    return s;
+  if ((s = cuda_status(cudaMemcpyAsync(root, fs->tree + (2 * leaves - 2) * 8, 32, cudaMemcpyDeviceToHost, fs->st),
+                       "root copy")))
+    return s;
+  if ((s = guard_enqueue(fs->ctx, fs->slot, fs->st))) return s;
+  if ((s = cuda_status(cudaStreamSynchronize(fs->st), "FRI shard round"))) return s;
+  return guard_verdict(fs->ctx, fs->slot);
+}
+
+}  // namespace
+
+extern "C" pico_status pico_gpu_fri_shard_begin(pico_ctx* ctx, pico_field field, const uint32_t* rows,
+                                                uint32_t log_n, uint32_t log_shards, uint32_t shard,
+                                                uint32_t flags, pico_fri_shard** out, uint32_t root[8]) {
+  if (out) *out = nullptr;
+  if (!ctx || !rows || !out || !root || (field != PICO_KOALABEAR && field != PICO_BABYBEAR)) {
+    set_error("fri_shard_begin: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  const uint32_t S = field == PICO_KOALABEAR ? 24u : 27u;
+  if (log_n > S || log_shards > 20 || log_n < log_shards + 1 || shard >= (1u << log_shards)) {
+    set_error("fri_shard_begin: codeword 2^%u in 2^%u shards (shard %u): each shard needs two rows", log_n,
+              log_shards, shard);
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (flags & ~PICO_INPUT_DEVICE) {
+    set_error("fri_shard_begin: unknown flags 0x%x", flags);
+    return PICO_ERR_INVALID_ARG;
+  }
+  auto fs = std::make_unique<pico_fri_shard>();
+  fs->ctx = ctx;
+  fs->field = field;
+  fs->log_len = log_n;
+  fs->log_shards = log_shards;
+  fs->shard = shard;
+  const uint32_t lr = log_n - log_shards;
+  const uint64_t b0 = ((16ull << lr) + 255) & ~255ull, b1 = ((16ull << (lr - 1)) + 255) & ~255ull;
+  const uint64_t bt = ((((2ull << (lr - 1)) - 1) * 32) + 255) & ~255ull;
+  fs->bytes = b0 + b1 + bt + 256;
+  if (!try_reserve(ctx, fs->bytes)) {
+    set_error("fri_shard_begin: HBM budget exceeded");
+    return PICO_ERR_OUT_OF_MEMORY;
+  }
+  cudaSetDevice(ctx->device);
+  fs->st = pick_stream(ctx, nullptr, &fs->slot);
+  pico_status s = device_alloc(&fs->block, fs->bytes, fs->st);
+  if (s) {
+    unreserve(ctx, fs->bytes);
+    return s;
+  }
+  uint8_t* p = (uint8_t*)fs->block;
+  fs->cw[0] = (uint32_t*)p;
+  fs->cw[1] = (uint32_t*)(p + b0);
+  fs->tree = (uint32_t*)(p + b0 + b1);
+  fs->d_beta = (uint32_t*)(p + b0 + b1 + bt);
+  // round 0: this shard's rows, their leaves (one permutation per row pair) and subtree
+  RowGroup g;
+  memset(&g, 0, sizeof g);
+  g.n_segs = 1;
+  g.total_width = 8;
+  g.segs[0].ptr = fs->cw[0];
+  g.segs[0].width = 8;
+  s = cuda_status(cudaMemcpyAsync(fs->cw[0], rows, 16ull << lr,
+                                  (flags & PICO_INPUT_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  fs->st),
+                  "codeword rows");
+  if (!s) s = cuda_status(launch_hash_rows(field, g, 1ull << (lr - 1), fs->tree, fs->st), "FRI leaf hashing");
+  if (!s) s = shard_tree_root(fs.get(), root);
+  if (s) {
+    cudaStreamSynchronize(fs->st);
+    cudaFreeAsync(fs->block, fs->st);
+    cudaStreamSynchronize(fs->st);
+    unreserve(ctx, fs->bytes);
+    return s;
+  }
+  *out = fs.release();
+  return PICO_OK;
+}
+
+extern "C" pico_status pico_gpu_fri_shard_fold(pico_fri_shard* fs, const uint32_t beta[4], uint32_t root[8]) {
+  if (!fs || !beta || !root) {
+    set_error("fri_shard_fold: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  if (fs->log_rows() < 2) {
+    set_error("fri_shard_fold: the shard holds 2^%u rows, too few to fold into a tree; gather the codeword",
+              fs->log_rows());
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(fs->ctx->device);
+  pico_status s;
+  if ((s = cuda_status(cudaMemcpyAsync(fs->d_beta, beta, 16, cudaMemcpyHostToDevice, fs->st), "beta"))) return s;
+  const uint64_t new_rows = 1ull << (fs->log_rows() - 1);
+  if ((s = cuda_status(launch_fri_fold_hash_rows(fs->field, fs->cw[fs->cur], fs->log_len, fs->shard * new_rows,
+                                                 new_rows / 2, fs->d_beta, twiddles(fs->ctx, fs->field),
+                                                 fs->cw[fs->cur ^ 1], fs->tree, fs->st),
+                       "shard fold and hash")))
+    return s;
+  fs->cur ^= 1;
+  fs->log_len--;
+  return shard_tree_root(fs, root);
+}
+
+extern "C" pico_status pico_gpu_fri_shard_rows(pico_fri_shard* fs, uint32_t* out, uint32_t flags) {
+  if (!fs || !out || (flags & ~PICO_OUTPUT_DEVICE)) {
+    set_error("fri_shard_rows: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(fs->ctx->device);
+  pico_status s = cuda_status(cudaMemcpyAsync(out, fs->cw[fs->cur], 16ull << fs->log_rows(),
+                                              (flags & PICO_OUTPUT_DEVICE) ? cudaMemcpyDeviceToDevice
+                                                                           : cudaMemcpyDeviceToHost,
+                                              fs->st),
+                              "shard rows");
+  if (s) return s;
+  return cuda_status(cudaStreamSynchronize(fs->st), "fri_shard_rows");
+}
+
+extern "C" pico_status pico_gpu_fri_shard_release(pico_fri_shard* fs) {
+  if (!fs) return PICO_OK;
+  cudaSetDevice(fs->ctx->device);
+  cudaFreeAsync(fs->block, fs->st);
+  pico_status s = cuda_status(cudaStreamSynchronize(fs->st), "fri_shard_release");
+  unreserve(fs->ctx, fs->bytes);
+  delete fs;
+  return s;
+}

@@ -119,6 +119,12 @@ cudaError_t launch_fri_fold_tw(int field, const uint32_t* cw, uint32_t log_len, 
 cudaError_t launch_fri_fold_hash(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,
                                  TwiddleTables tw, uint32_t* out, const uint32_t* inject, uint32_t* leaves,
                                  cudaStream_t st);
+// One shard of a codeword split by rows: cw holds the 4 n_leaves rows from
+// row 2 row0 of a 2^log_len-row codeword; fold them (twiddles of their rows in
+// the whole codeword) into out (2 n_leaves rows) and hash the leaves.
+cudaError_t launch_fri_fold_hash_rows(int field, const uint32_t* cw, uint32_t log_len, uint64_t row0,
+                                      uint64_t n_leaves, const uint32_t* beta, TwiddleTables tw, uint32_t* out,
+                                      uint32_t* leaves, cudaStream_t st);
 // Coefficients of the final polynomial (2^log_keep x 4 words) from the last
 // codeword of 2^log_len EF4 elements; *err set if higher coefficients are nonzero.
 cudaError_t launch_fri_final_poly(int field, const uint32_t* cw, uint32_t log_len, uint32_t log_keep,

@@ -376,15 +376,17 @@ cudaError_t launch_compress(int field, const uint32_t* prev, uint32_t* next, uin
 // vm/src/compiler/recursion/circuit/fri.rs:345-377): row r of the (len/2) x 2
 // matrix (lo, hi) folds to
 //   (lo + hi)/2 + (beta/2) * g_inv^rev(r) * (lo - hi),
-// g = two_adic_generator(log len), rev over log(len/2) bits.
+// g = two_adic_generator(log len), rev over log(len/2) bits.  The pair is read
+// at rows 2r, 2r+1 of cw; rg is its row in the whole codeword (r itself,
+// except for one shard of a codeword split by rows).
 template <class F>
 __device__ __forceinline__ Ext4 fri_fold_row(const uint32_t* cw, uint32_t log_len, uint64_t r, const Ext4& hb,
-                                             const TwiddleTables& tw) {
+                                             const TwiddleTables& tw, uint64_t rg) {
   using B = Fp<F>;
   using E = Ef<F>;
-  // g_inv^rev(r) = w_max^(-(rev(r) << (S - log_len)))
+  // g_inv^rev(rg) = w_max^(-(rev(rg) << (S - log_len)))
   const uint32_t mask = (1u << F::TWO_ADICITY) - 1u;
-  uint32_t e = (uint32_t)bitrev64(r, (int)log_len - 1) << (F::TWO_ADICITY - log_len);
+  uint32_t e = (uint32_t)bitrev64(rg, (int)log_len - 1) << (F::TWO_ADICITY - log_len);
   e = (0u - e) & mask;
   uint32_t t = B::mul(__ldg(tw.hi + (e >> 14)), __ldg(tw.lo + (e & 0x3fffu)));
   const uint4 lo4 = __ldg(reinterpret_cast<const uint4*>(cw) + 2 * r);
@@ -412,7 +414,7 @@ __global__ void k_fri_fold(const uint32_t* cw, uint32_t log_len, const uint32_t*
   const uint64_t h = 1ull << (log_len - 1);
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= h) return;
-  Ext4 res = fri_fold_row<F>(cw, log_len, r, half_beta<F>(beta), tw);
+  Ext4 res = fri_fold_row<F>(cw, log_len, r, half_beta<F>(beta), tw, r);
   if (inject) {
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(inject) + r);
     res = Ef<F>::add(res, Ext4{{v.x, v.y, v.z, v.w}});
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(256) k_fri_fold_hash(const uint32_t* cw, uint3
 #pragma unroll
   for (int u = 0; u < 2; u++) {
     const uint64_t r = 2 * k + u;
-    Ext4 res = fri_fold_row<F>(cw, log_len, r, hb, tw);
+    Ext4 res = fri_fold_row<F>(cw, log_len, r, hb, tw, r);
     if (inject) {
       const uint4 v = __ldg(reinterpret_cast<const uint4*>(inject) + r);
       res = Ef<F>::add(res, Ext4{{v.x, v.y, v.z, v.w}});
@@ -450,6 +452,48 @@ __global__ void __launch_bounds__(256) k_fri_fold_hash(const uint32_t* cw, uint3
   uint4* lp = reinterpret_cast<uint4*>(leaves + 8 * k);
   lp[0] = make_uint4(s[0], s[1], s[2], s[3]);
   lp[1] = make_uint4(s[4], s[5], s[6], s[7]);
+}
+
+// One shard's part of k_fri_fold_hash for a codeword split by rows: the
+// shard holds rows [2 row0, 2 row0 + 4 n_leaves) of the 2^log_len-row
+// codeword at cw; it folds them into rows [row0, row0 + 2 n_leaves) (stored
+// from out) and hashes their n_leaves leaves.
+template <class F>
+__global__ void __launch_bounds__(256) k_fri_fold_hash_rows(const uint32_t* cw, uint32_t log_len, uint64_t row0,
+                                                            uint64_t n_leaves, const uint32_t* beta,
+                                                            TwiddleTables tw, uint32_t* out, uint32_t* leaves) {
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= n_leaves) return;
+  const Ext4 hb = half_beta<F>(beta);
+  uint32_t s[16];
+#pragma unroll
+  for (int u = 0; u < 2; u++) {
+    const uint64_t r = 2 * k + u;
+    const Ext4 res = fri_fold_row<F>(cw, log_len, r, hb, tw, row0 + r);
+    reinterpret_cast<uint4*>(out)[r] = make_uint4(res.c[0], res.c[1], res.c[2], res.c[3]);
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[4 * u + i] = res.c[i];
+  }
+#pragma unroll
+  for (int i = 8; i < 16; i++) s[i] = 0;
+  p2_permute<F>(s);
+  uint4* lp = reinterpret_cast<uint4*>(leaves + 8 * k);
+  lp[0] = make_uint4(s[0], s[1], s[2], s[3]);
+  lp[1] = make_uint4(s[4], s[5], s[6], s[7]);
+}
+
+cudaError_t launch_fri_fold_hash_rows(int field, const uint32_t* cw, uint32_t log_len, uint64_t row0,
+                                      uint64_t n_leaves, const uint32_t* beta, TwiddleTables tw, uint32_t* out,
+                                      uint32_t* leaves, cudaStream_t st) {
+  if (n_leaves == 0) return cudaSuccess;
+  if (log_len < 2 || 2 * (row0 + 2 * n_leaves) > (1ull << log_len)) return cudaErrorInvalidValue;
+  if (field == 0)
+    k_fri_fold_hash_rows<KoalaBear><<<blocks_for(n_leaves, 256), 256, 0, st>>>(cw, log_len, row0, n_leaves, beta,
+                                                                               tw, out, leaves);
+  else
+    k_fri_fold_hash_rows<BabyBear><<<blocks_for(n_leaves, 256), 256, 0, st>>>(cw, log_len, row0, n_leaves, beta,
+                                                                              tw, out, leaves);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fri_fold_hash(int field, const uint32_t* cw, uint32_t log_len, const uint32_t* beta,

@@ -590,3 +590,50 @@ def test_row_split_commit_with_extension_traces(gpu, orc, f):
     want, _, _ = orc.pcs_commit(f, flat, [F.lde_shift(f)] * 2, b)
     subs = [pcs.commit_shard(items, k, s, keep=False)[0] for s in range(1 << k)]
     assert merkle_top(f, np.stack(subs)).tolist() == want.tolist()
+
+
+@pytest.mark.parametrize("f,k,lf", [(0, 1, 0), (1, 2, 0), (0, 2, 4), (1, 3, 2)])
+def test_fri_row_split_matches_one_device(gpu, orc, f, k, lf):
+    """The FRI commit phase split by rows over 2^k shards (every shard on this
+    GPU in turn, as 2^k ranks would run them side by side): roots, betas,
+    final polynomial and the challenger afterwards equal the one-device
+    phase's and the oracle's."""
+    from pico_b200.pcs import new_challenger
+    from pico_b200.sharded import fri_commit_phase_split
+
+    cw = orc.coset_lde(f, F.random_matrix(f, 13, 4, 9700 + f), 1, F.lde_shift(f))  # 2^14 EF4 rows
+    pcs = TwoAdicFriPcs(gpu, f, 1)
+    roots, betas, final, ch = fri_commit_phase_split(pcs, cw, k, log_final_len=lf, min_log_rows=4)
+    want_r, want_b, want_f, want_ch = orc.fri_commit_phase(f, cw, 1, lf)
+    assert np.array_equal(roots, want_r) and np.array_equal(betas, want_b)
+    assert np.array_equal(final, want_f)
+    one_ch = new_challenger()
+    one = pcs.fri_commit_phase(cw, log_final_len=lf, challenger=one_ch)
+    assert np.array_equal(one.roots, roots) and np.array_equal(one.betas, betas)
+    assert bytes(one_ch) == bytes(ch)
+    assert gpu.memory()[0] == 0
+
+
+def test_fri_sharded_over_a_one_rank_group(orc):
+    """fri_commit_phase_sharded through a one-rank gloo group (its gathers
+    included): the one shard folds on the device until 2^4 rows remain."""
+    import socket
+
+    import torch.distributed as dist
+
+    from pico_b200.sharded import fri_commit_phase_sharded
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    ctx = GpuContext(0)
+    try:
+        f = 0
+        cw = orc.coset_lde(f, F.random_matrix(f, 11, 4, 9750), 1, F.lde_shift(f))
+        roots, betas, final, _ = fri_commit_phase_sharded(TwoAdicFriPcs(ctx, f, 1), cw, 12, min_log_rows=4)
+        want_r, want_b, want_f, _ = orc.fri_commit_phase(f, cw, 1, 0)
+        assert np.array_equal(roots, want_r) and np.array_equal(betas, want_b) and np.array_equal(final, want_f)
+    finally:
+        ctx.close()
+        dist.destroy_process_group()
