@@ -255,6 +255,13 @@ pico_status pico_gpu_commit_shard(pico_ctx *ctx, pico_field field, const pico_ma
  * shard roots (8 words each, in shard order) compressed pairwise up to the
  * root (MerkleTreeMmcs compression; no device needed). */
 pico_status pico_gpu_merkle_top(pico_field field, const uint32_t *roots, uint32_t log_shards, uint32_t root[8]);
+/* The last log_shards digests of a Merkle path through shard `shard` of a
+ * row-split commit (lowest level first): pico_gpu_open_batch on the shard's
+ * prover data, at the index's row within the shard, gives the opened rows and
+ * the path up to the shard's root; these siblings complete the path of the
+ * whole commit (Mmcs::open_batch, checked as fri.rs:389-436 checks it). */
+pico_status pico_gpu_merkle_top_path(pico_field field, const uint32_t *roots, uint32_t log_shards, uint32_t shard,
+                                     uint32_t *path);
 /* Poseidon2KoalaBear<16> / Poseidon2BabyBear<16> on n states of 16 words, in place. */
 pico_status pico_gpu_poseidon2_permute(pico_ctx *ctx, pico_field field, uint32_t *states, uint64_t n,
                                        uint32_t flags);

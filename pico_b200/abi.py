@@ -168,6 +168,7 @@ SIGNATURES = {
     "pico_gpu_commit_shard": (C.c_int, [_vp, C.c_int, C.POINTER(Matrix), _u32, _u32, _u32, _u32, _u32,
                                         C.POINTER(_vp), _u32p]),
     "pico_gpu_merkle_top": (C.c_int, [C.c_int, _u32p, _u32, _u32p]),
+    "pico_gpu_merkle_top_path": (C.c_int, [C.c_int, _u32p, _u32, _u32, _u32p]),
     "pico_gpu_fri_shard_begin": (C.c_int, [_vp, C.c_int, _vp, _u32, _u32, _u32, _u32, C.POINTER(_vp), _u32p]),
     "pico_gpu_fri_shard_fold": (C.c_int, [_vp, _u32p, _u32p]),
     "pico_gpu_fri_shard_rows": (C.c_int, [_vp, _vp, _u32]),

@@ -1469,6 +1469,30 @@ extern "C" pico_status pico_gpu_merkle_top(pico_field field, const uint32_t* roo
   return PICO_OK;
 }
 
+// The siblings of shard s's subtree root on its way up the top levels:
+// level k's sibling is root s ^ 1, then the sibling of each parent.
+extern "C" pico_status pico_gpu_merkle_top_path(pico_field field, const uint32_t* roots, uint32_t log_shards,
+                                                uint32_t shard, uint32_t* path) {
+  if ((field != PICO_KOALABEAR && field != PICO_BABYBEAR) || !roots || (log_shards && !path) || log_shards > 20 ||
+      shard >= (1u << log_shards)) {
+    set_error("merkle_top_path: bad arguments");
+    return PICO_ERR_INVALID_ARG;
+  }
+  std::vector<uint32_t> level(roots, roots + (8ull << log_shards));
+  uint32_t idx = shard;
+  for (uint32_t l = log_shards; l > 0; l--) {
+    memcpy(path + 8ull * (log_shards - l), &level[8ull * (idx ^ 1)], 32);
+    for (uint64_t i = 0; i < (1ull << (l - 1)); i++) {
+      uint32_t s[16];
+      memcpy(s, &level[16 * i], 64);
+      host_permute(field, s);
+      memcpy(&level[8 * i], s, 32);
+    }
+    idx >>= 1;
+  }
+  return PICO_OK;
+}
+
 extern "C" pico_status pico_gpu_commit_stats(const pico_commit* c, pico_commit_stats* out) {
   if (!c || !out) {
     set_error("commit_stats: bad arguments");

@@ -557,3 +557,15 @@ def merkle_top(field, shard_roots) -> np.ndarray:
     abi.check(abi.load().pico_gpu_merkle_top(F.field_id(field), roots.ctypes.data_as(C.POINTER(C.c_uint32)), k,
                                              out.ctypes.data_as(C.POINTER(C.c_uint32))))
     return out
+
+
+def merkle_top_path(field, shard_roots, shard: int) -> np.ndarray:
+    """The siblings above shard `shard`'s subtree root, lowest first
+    (pico_gpu_merkle_top_path): appended to the shard's own open_batch path,
+    the path through the whole row-split commit."""
+    roots = np.ascontiguousarray(np.asarray(shard_roots, dtype=np.uint32).reshape(-1, 8))
+    k = _log2_exact(roots.shape[0])
+    out = np.zeros((k, 8), dtype=np.uint32)
+    abi.check(abi.load().pico_gpu_merkle_top_path(F.field_id(field), roots.ctypes.data_as(C.POINTER(C.c_uint32)), k,
+                                                  shard, out.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return out

@@ -637,3 +637,32 @@ def test_fri_sharded_over_a_one_rank_group(orc):
     finally:
         ctx.close()
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("f,b,k", [(0, 1, 1), (1, 2, 2)])
+def test_row_split_open_batch(gpu, f, b, k):
+    """Mmcs::open_batch of a row-split commit: the owning shard's open_batch at
+    the index's row within the shard, plus merkle_top_path over the shard
+    roots, equals open_batch on the whole commit (rows and path)."""
+    from pico_b200.pcs import merkle_top_path
+
+    shapes = [(11, 3), (9, 5), (11, 2), (4, 1)]
+    mats = [F.random_matrix(f, lh, w, 9800 + 5 * i + f) for i, (lh, w) in enumerate(shapes)]
+    pcs = TwoAdicFriPcs(gpu, f, b)
+    items = [(pcs.natural_domain_for_degree(m.shape[0]), m) for m in mats]
+    _, full = pcs.commit(items)
+    shards = [pcs.commit_shard(items, k, s) for s in range(1 << k)]
+    roots = np.stack([r for r, _ in shards])
+    mmcs = MerkleTreeMmcs(gpu, f)
+    log_max = 11 + b
+    rng = np.random.default_rng(3)
+    for index in list(rng.integers(0, 1 << log_max, size=12)) + [0, (1 << log_max) - 1]:
+        index = int(index)
+        s, local = index >> (log_max - k), index & ((1 << (log_max - k)) - 1)
+        rows, path = mmcs.open_batch(local, shards[s][1])
+        want_rows, want_path = mmcs.open_batch(index, full)
+        assert all(np.array_equal(a, w) for a, w in zip(rows, want_rows))
+        assert np.array_equal(np.concatenate([path, merkle_top_path(f, roots, s)]), want_path)
+    for _, pd in shards:
+        pd.release()
+    full.release()

@@ -97,3 +97,20 @@ def test_merkle_top_refuses_bad_arguments():
         merkle_top(0, np.zeros((3, 8), dtype=np.uint32))  # not a power of two
     with pytest.raises(PicoError):
         merkle_top(7, np.zeros((2, 8), dtype=np.uint32))  # unknown field
+
+
+@pytest.mark.parametrize("f,b,k", [(0, 1, 1), (1, 2, 2)])
+def test_merkle_top_path_is_the_upper_path(orc, f, b, k):
+    """pico_gpu_merkle_top_path: the siblings of shard s's subtree root up to
+    the root, the last k digests of every Merkle path through that shard."""
+    from pico_b200 import fields as F
+    from pico_b200.pcs import merkle_top_path
+
+    mats = _traces(f)
+    _, _, layers = orc.pcs_commit(f, mats, [F.lde_shift(f)] * len(mats), b, want_layers=True)
+    depth = lambda d: layers[len(layers) - (2 << d) + 1: len(layers) - (1 << d) + 1]
+    roots = depth(k)
+    for s in range(1 << k):
+        want = np.stack([depth(d)[(s >> (k - d)) ^ 1] for d in range(k, 0, -1)])
+        assert np.array_equal(merkle_top_path(f, roots, s), want)
+    assert merkle_top_path(f, roots[:1], 0).shape == (0, 8)
