@@ -12,9 +12,13 @@ give every rank the commitment root.  Rank r of the group computes shard r.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
-from .pcs import merkle_top
+from . import abi
+from . import fields as F
+from .pcs import _is_device, _ptr, merkle_top, new_challenger
 
 
 def _log2_world(world: int) -> int:
@@ -59,12 +63,6 @@ class FriShard:
     2^log_n-row EF4 codeword, (rows, 4) Monty words, host or device."""
 
     def __init__(self, ctx, field, rows, log_n: int, log_shards: int, shard: int):
-        import ctypes as C
-
-        from . import abi
-        from . import fields as F
-        from .pcs import _is_device, _ptr
-
         self.ctx, self.field = ctx, F.field_id(field)
         self.log_len, self.log_shards = log_n, log_shards
         self.root = np.zeros(8, dtype=np.uint32)
@@ -81,10 +79,6 @@ class FriShard:
         return self.log_len - self.log_shards
 
     def fold(self, beta) -> np.ndarray:
-        import ctypes as C
-
-        from . import abi
-
         b = np.ascontiguousarray(beta, dtype=np.uint32).reshape(4)
         abi.check(self.ctx.lib.pico_gpu_fri_shard_fold(self.handle, b.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                        self.root.ctypes.data_as(C.POINTER(C.c_uint32))))
@@ -92,35 +86,23 @@ class FriShard:
         return self.root
 
     def rows(self) -> np.ndarray:
-        from . import abi
-
         out = np.zeros((1 << self.log_rows(), 4), dtype=np.uint32)
         abi.check(self.ctx.lib.pico_gpu_fri_shard_rows(self.handle, out.ctypes.data, 0))
         return out
 
     def release(self):
-        from . import abi
-
         if self.handle:
             abi.check(self.ctx.lib.pico_gpu_fri_shard_release(self.handle))
             self.handle = None
 
 
 def _observe(field, ch, words):
-    import ctypes as C
-
-    from . import abi
-
     w = np.ascontiguousarray(words, dtype=np.uint32).reshape(-1)
     abi.check(abi.load().pico_gpu_challenger_observe(field, C.byref(ch), w.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                      w.size))
 
 
 def _sample(field, ch, n: int) -> np.ndarray:
-    import ctypes as C
-
-    from . import abi
-
     out = np.zeros(n, dtype=np.uint32)
     abi.check(abi.load().pico_gpu_challenger_sample(field, C.byref(ch), out.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                     n))
@@ -134,8 +116,6 @@ def _split_rounds(pcs, log_n: int, k: int, shard_roots, fold, codeword, log_fina
     beta sampled (the prover's DuplexChallenger, on the host) and every shard
     folded; then the short codeword gathered and the rest of the phase run on
     this device by pcs.fri_commit_phase with the same challenger."""
-    from .pcs import new_challenger
-
     f = pcs.field
     ch = challenger if challenger is not None else new_challenger()
     roots, betas = [], []
