@@ -752,6 +752,23 @@ def run_open(args, rank, world, local):
 
 
 # ---------------------------------------------------------------- FRI leg
+def fri_launches(log_n: int, rounds: int, log_final_len: int) -> int:
+    """Kernels one commit phase launches (the round loop of fri_host.cu): the
+    first round's leaf hashing; per round the wide compression levels one
+    launch each, seven narrow levels per subtree launch, the tree top with the
+    challenger step, and the fold (with the next leaves); then the final
+    observation (and the final polynomial when it keeps coefficients)."""
+    nl = 0
+    for r in range(rounds):
+        n = 1 << (log_n - r - 1)
+        nl += 1 if r == 0 else 0
+        while n > 512:
+            nl += 1
+            n = n >> 7 if n <= (1 << 15) else n // 2
+        nl += 2
+    return nl + (1 if log_final_len == 0 else 2)
+
+
 def run_fri(args):
     """FRI commit phase on a device-resident KoalaBear EF4 codeword of 2^23
     evaluations (a degree < 2^22 random polynomial, coset LDE with blowup 2):
@@ -837,6 +854,7 @@ def run_fri(args):
                    "l2": "codeword 128 MiB and its layers exceed L2 (126 MB); no flush"},
         "modes": out,
         "clocks": clocks,
+        "gpu_launches": args.steps * fri_launches(log_trace + b, rounds, 0),
         "e2e": {"value": n_el / e2e_s, "unit": "elements/s", "ms_per_step": e2e_s * 1e3,
                 "h2d_bytes_per_step": n_el * 16, "d2h_bytes_per_step": rounds * 48 + 16},
         "roofline": {"kernel": "the phase's Poseidon2 kernels (k_fri_fold_hash, k_compress, k_subtree_quad, "
