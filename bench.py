@@ -528,6 +528,7 @@ def c1_summary(ctx, args, local):
 
     from pico_b200 import TwoAdicDomain, TwoAdicFriPcs
     from pico_b200 import fields as F
+    from pico_b200.pcs import last_commit_stats
 
     wl = WORKLOADS[C1_WORKLOAD]
     field, b, shapes, seed = wl["field"], wl["log_blowup"], wl["shapes"](), wl["seed"]
@@ -552,13 +553,16 @@ def c1_summary(ctx, args, local):
             e1.synchronize()
             groups.append(e0.elapsed_time(e1) / (C1_STEPS // 5))
         out[tag] = (float(np.median(groups)), root.tolist(), [round(g, 4) for g in groups])
+        if tag == "host":
+            last = last_commit_stats()  # the last commit's own device timeline
+            host_phases = {"h2d_ms": last["h2d_ms"], "device_total_ms": last["total_ms"]}
     cpu = run_cpu(shapes, field, b, seed, 5, 1, max_cells=cells)
     ms_dev, ms_e2e = out["device"][0], out["host"][0]
     return {
         "workload": C1_WORKLOAD, "trace_cells": cells, "log_blowup": b, "steps": C1_STEPS,
         "value": cells / (ms_dev / 1e3), "ms_per_step": ms_dev,
         "e2e": {"value": cells / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e,
-                "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 32},
+                "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 32, **host_phases},
         "cpu_baseline": cpu,
         "gpu_over_cpu": cells / (ms_dev / 1e3) / cpu["value"],
         "gpu_over_cpu_e2e": cells / (ms_e2e / 1e3) / cpu["value"],
